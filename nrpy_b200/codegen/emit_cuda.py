@@ -1,0 +1,271 @@
+"""Emit CUDA device code for one pointwise BSSN kernel from SymPy expressions.
+
+Own code generator (not NRPy's c_codegen): it takes the expression lists assembled in
+``bssn_exprs`` and writes a templated ``__device__`` function that evaluates them at one
+grid point. Structure of the emitted body:
+
+1. Common subexpressions come from ``sympy.cse``.
+2. Every leaf symbol (gridfunction value, finite-difference derivative, rfm precompute
+   value, parameter) is defined lazily, right before the first statement that reads it,
+   to keep register live ranges short.
+3. Finite differences read stencil points through the ``LD(gf, d0, d1, d2)`` macro that
+   the including translation unit defines (global loads or shared-memory tiles), so the
+   same algebra serves several kernel layouts.
+
+Derivative symbol grammar (the names NRPy's equation modules use, c_codegen.py:752-1140):
+``<gf>_d<kind><indices>`` with kind in {D, DD, upD, KOD}; the first ``rank(gf)`` digits
+are the gridfunction's component indices and the rest are derivative directions.
+Upwinded derivatives select, per direction, the stencil shifted toward the upwind side
+(``UPWIND_ALG(v) = v > 0``, nrpy/helpers/cuda_intrinsics.h:43) using the control vector
+betaU[i] = vetU[i] * ReU[i].
+"""
+
+import re
+from typing import Dict, List, Optional, Sequence, Set, Tuple
+
+import sympy as sp
+from sympy.printing.c import C99CodePrinter
+
+from . import fdcoeffs as fdc
+from .bssn_exprs import GF_ORDER, RBAR_ORDER
+
+GF_INDEX = {g: i for i, g in enumerate(GF_ORDER)}
+RBAR_INDEX = {g: i for i, g in enumerate(RBAR_ORDER)}
+BASE_RANK = {"aDD": 2, "hDD": 2, "vetU": 1, "betU": 1, "lambdaU": 1, "alpha": 0, "cf": 0, "trK": 0}
+DERIV_RE = re.compile(r"^(aDD|hDD|vetU|betU|lambdaU|alpha|cf|trK)_d(upD|KOD|DD|D)(\d+)$")
+RFM_FIELDS = {
+    "f0_of_xx0": ("rfm_f0", 0),
+    "f0_of_xx0__D0": ("rfm_f0_D0", 0),
+    "f0_of_xx0__DD00": ("rfm_f0_DD00", 0),
+    "f0_of_xx0__DDD000": ("rfm_f0_DDD000", 0),
+    "f1_of_xx1": ("rfm_f1", 1),
+    "f1_of_xx1__D1": ("rfm_f1_D1", 1),
+    "f1_of_xx1__DD11": ("rfm_f1_DD11", 1),
+}
+SCALAR_PARAMS = {"eta", "KreissOliger_strength_gauge", "KreissOliger_strength_nongauge"}
+
+
+def parse_deriv(name: str) -> Optional[Tuple[str, str, Tuple[int, ...]]]:
+    m = DERIV_RE.match(name)
+    if not m:
+        return None
+    base, kind, digits = m.groups()
+    rank = BASE_RANK[base]
+    comp = digits[:rank]
+    dirs = tuple(int(c) for c in digits[rank:])
+    want = 2 if kind == "DD" else 1
+    if len(dirs) != want:
+        raise ValueError(f"cannot parse derivative symbol {name}")
+    return base + comp, kind, dirs
+
+
+def off_name(o: int) -> str:
+    return "0" if o == 0 else (f"p{o}" if o > 0 else f"m{-o}")
+
+
+class _Printer(C99CodePrinter):
+    """C++ printer: algebra type ``T``, integer powers as products, no libm pow()."""
+
+    def __init__(self, names: Dict[str, str]):
+        super().__init__({"math_macros": {}})
+        self._names = names
+
+    def _print_Symbol(self, expr):
+        n = expr.name
+        return self._names.get(n, n)
+
+    def _print_Rational(self, expr):
+        p, q = int(expr.p), int(expr.q)
+        if q == 1:
+            return f"T({p}.0)"
+        return f"T({p}.0/{q}.0)"
+
+    def _print_Integer(self, expr):
+        return f"T({int(expr)}.0)"
+
+    def _print_Float(self, expr):
+        return f"T({repr(float(expr))})"
+
+    def _print_Pow(self, expr):
+        b, e = expr.base, expr.exp
+        bs = self.parenthesize(b, 100)
+        if e.is_Integer:
+            n = int(e)
+            if n == 0:
+                return "T(1.0)"
+            mag = abs(n)
+            prod = "*".join([bs] * mag) if mag <= 4 else f"ipow({self._print(b)}, {mag})"
+            if mag > 1:
+                prod = f"({prod})"
+            return prod if n > 0 else f"(T(1.0)/{prod})"
+        if e == sp.Rational(1, 2):
+            return f"sqrt({self._print(b)})"
+        if e == sp.Rational(-1, 2):
+            return f"(T(1.0)/sqrt({self._print(b)}))"
+        if e == sp.Rational(1, 3):
+            return f"cbrt({self._print(b)})"
+        if e == sp.Rational(-1, 3):
+            return f"(T(1.0)/cbrt({self._print(b)}))"
+        if e == sp.Rational(2, 3):
+            return f"(cbrt({self._print(b)})*cbrt({self._print(b)}))"
+        raise NotImplementedError(f"power {expr}")
+
+    def _print_Function(self, expr):
+        fname = expr.func.__name__
+        if fname == "nrpyAbs":
+            return f"fabs({self._print(expr.args[0])})"
+        return super()._print_Function(expr)
+
+    def _print_Abs(self, expr):
+        return f"fabs({self._print(expr.args[0])})"
+
+
+class PointKernel:
+    """Collects leaf definitions and CSE'd statements for one pointwise function."""
+
+    def __init__(self, symmetry_axes: str = ""):
+        self.sym_axes = {int(c) for c in symmetry_axes}
+        self.lines: List[str] = []
+        self.defined: Set[str] = set()
+        self.loaded: Set[Tuple[str, Tuple[int, int, int]]] = set()
+        self.names: Dict[str, str] = {}
+        self.upwind_vec: Optional[List[sp.Expr]] = None
+        self.printer = _Printer(self.names)
+        self.stats = {"loads": 0, "derivs": 0}
+
+    # ---- leaves -----------------------------------------------------------------
+    def _load(self, gf: str, off: Tuple[int, int, int]) -> str:
+        var = f"v_{gf}_{off_name(off[0])}_{off_name(off[1])}_{off_name(off[2])}"
+        if (gf, off) not in self.loaded:
+            self.loaded.add((gf, off))
+            self.stats["loads"] += 1
+            self.lines.append(f"const double {var} = LD({GF_INDEX[gf]}, {off[0]}, {off[1]}, {off[2]});")
+        return var
+
+    def _pt(self, gf: str, d: int, o: int, d2: int = -1, o2: int = 0) -> str:
+        off = [0, 0, 0]
+        off[d] += o
+        if d2 >= 0:
+            off[d2] += o2
+        return self._load(gf, tuple(off))
+
+    def _define_leaf(self, name: str) -> None:
+        if name in self.defined:
+            return
+        self.defined.add(name)
+        if name in GF_INDEX:
+            v = self._load(name, (0, 0, 0))
+            self.lines.append(f"const T {name} = T({v});")
+            return
+        if name in RBAR_INDEX:
+            self.lines.append(f"const T {name} = T(LDAUX({RBAR_INDEX[name]}));")
+            return
+        if name in RFM_FIELDS:
+            arr, d = RFM_FIELDS[name]
+            self.lines.append(f"const T {name} = T(RFM({arr}, {d}));")
+            return
+        if name in SCALAR_PARAMS:
+            self.lines.append(f"const T {name} = T(PARAM({name}));")
+            return
+        pd = parse_deriv(name)
+        if pd is None:
+            raise KeyError(f"unknown symbol {name}")
+        gf, kind, dirs = pd
+        self.stats["derivs"] += 1
+        self.lines.append(self._deriv_code(name, gf, kind, dirs))
+
+    def _deriv_code(self, name: str, gf: str, kind: str, dirs: Tuple[int, ...]) -> str:
+        P = self.printer
+        if kind == "D":
+            (d,) = dirs
+            w = fdc.first_centred()
+            terms = []
+            for o in sorted(k for k in w if k > 0):
+                terms.append(f"{P._print(w[o])}*(T({self._pt(gf, d, o)}) - T({self._pt(gf, d, -o)}))")
+            return f"const T {name} = T(invdxx{d}) * ({' + '.join(terms)});"
+        if kind == "DD":
+            d1, d2 = dirs
+            if d1 == d2:
+                w = fdc.second_centred()
+                terms = [f"{P._print(w[0])}*T({self._pt(gf, d1, 0)})"]
+                for o in sorted(k for k in w if k > 0):
+                    terms.append(f"{P._print(w[o])}*(T({self._pt(gf, d1, o)}) + T({self._pt(gf, d1, -o)}))")
+                return f"const T {name} = T(invdxx{d1})*T(invdxx{d1}) * ({' + '.join(terms)});"
+            w = fdc.first_centred()
+            pos = sorted(k for k in w if k > 0)
+
+            def inner(a: int) -> str:
+                return " + ".join(
+                    f"{P._print(w[b])}*(T({self._pt(gf, d1, a, d2, b)}) - T({self._pt(gf, d1, a, d2, -b)}))"
+                    for b in pos
+                )
+
+            outer = " + ".join(f"{P._print(w[a])}*(({inner(a)}) - ({inner(-a)}))" for a in pos)
+            return f"const T {name} = T(invdxx{d1})*T(invdxx{d2}) * ({outer});"
+        if kind == "upD":
+            (d,) = dirs
+            up = fdc.upwind(+1)
+            # downwind weights satisfy dn[s] = -up[-s]: select the sample, not the weight.
+            terms = []
+            for t in sorted(up):
+                fu = self._pt(gf, d, t)
+                fd = self._pt(gf, d, -t)
+                terms.append(f"{P._print(up[t])}*(Upwind{d} ? T({fu}) : -T({fd}))")
+            return f"const T {name} = T(invdxx{d}) * ({' + '.join(terms)});"
+        if kind == "KOD":
+            (d,) = dirs
+            w = fdc.kreiss_oliger()
+            terms = [f"{P._print(w[0])}*T({self._pt(gf, d, 0)})"]
+            for o in sorted(k for k in w if k > 0):
+                terms.append(f"{P._print(w[o])}*(T({self._pt(gf, d, o)}) + T({self._pt(gf, d, -o)}))")
+            return f"const T {name} = T(invdxx{d}) * ({' + '.join(terms)});"
+        raise ValueError(kind)
+
+    def _ensure(self, expr: sp.Expr) -> None:
+        for s in sorted(expr.free_symbols, key=lambda x: x.name):
+            if s.name.startswith("_cse"):
+                continue
+            if parse_deriv(s.name) and parse_deriv(s.name)[1] == "upD":
+                self._ensure_upwind()
+            self._define_leaf(s.name)
+
+    def _ensure_upwind(self) -> None:
+        if "Upwind0" in self.defined:
+            return
+        self.defined.add("Upwind0")
+        assert self.upwind_vec is not None
+        for i, e in enumerate(self.upwind_vec):
+            self._ensure(e)
+            self.lines.append(f"const bool Upwind{i} = ({self.printer._print(e)}) > T(0.0);")
+
+    # ---- driver -------------------------------------------------------------------
+    def build(self, outputs: Sequence[Tuple[str, sp.Expr]], upwind_vec=None) -> str:
+        self.upwind_vec = upwind_vec
+        exprs = [sp.sympify(e) for _, e in outputs]
+        syms = (sp.Symbol(f"_cse{i}") for i in range(10**7))
+        repl, reduced = sp.cse(exprs, symbols=syms, order="none")
+        for s, e in repl:
+            self._ensure(e)
+            self.lines.append(f"const T {s.name} = {self.printer._print(e)};")
+        for (lhs, _), e in zip(outputs, reduced):
+            self._ensure(e)
+            self.lines.append(f"{lhs} = {self.printer._print(e)};")
+        return "\n".join("  " + ln for ln in self.lines)
+
+
+def emit_point_function(
+    fname: str,
+    outputs: Sequence[Tuple[str, sp.Expr]],
+    upwind_vec=None,
+    symmetry_axes: str = "",
+    comment: str = "",
+) -> Tuple[str, Dict[str, int]]:
+    pk = PointKernel(symmetry_axes)
+    body = pk.build(outputs, upwind_vec)
+    head = f"// {comment}\n" if comment else ""
+    code = (
+        f"{head}template <typename T, typename Ctx>\n"
+        f"__device__ __forceinline__ void {fname}(const Ctx &ctx, T *__restrict__ out) {{\n"
+        f"{body}\n}}\n"
+    )
+    return code, dict(pk.stats)
