@@ -1,0 +1,326 @@
+"""Benchmark: BSSN RK4 grid-point updates/s on B200 (libbssn_b200), with the reference's
+CPU implementation timed beside it.
+
+Workload (one "step" = one full RK4 step, MoL_step_forward_in_time): SinhSpherical
+256x64x64 interior (+3 ghost zones), AMPL=10, SINHW=0.2, Brill-Lindquist masses
+~U[0.3,0.7] and z = +/-U[0.3,0.8] from the seed, FP64 state, 4th-order FD, KO dissipation,
+outgoing-radiation outer BCs, Hamiltonian-constraint L2 every 20 steps (inside the
+timed region). Synthetic data: the Brill-Lindquist initial data computed in-process.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 (under torchrun): independent replicas, one per GPU (a single evolution does not
+shard without a halo exchange), each with its own seed; value is the
+whole-job rate = sum of all ranks' point updates / max over ranks of the device time.
+"""
+
+import argparse
+import ctypes as C
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+NXX = (256, 64, 64)
+AMPL, SINHW = 10.0, 0.2
+H_EVERY = 20
+B_ALG_PER_PT_STEP = 3072  # bytes: classic RK4 with an accumulator, each stage read once
+STAGE_WORDS = (72, 120, 120, 72)  # per interior point, FP64 words, stages 1..4
+METRIC = "BSSN RK4 grid-point updates/s on 1 B200, FP64 vs mixed at equal H-error"
+UNIT = "pt-updates/s"
+
+
+def bl_params(seed: int):
+    rng = np.random.default_rng(seed)
+    m1, m2 = rng.uniform(0.3, 0.7, 2)
+    z1, z2 = rng.uniform(0.3, 0.8), -rng.uniform(0.3, 0.8)
+    return float(m1), float(z1), float(m2), float(z2)
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(steps_wanted: int, warmup: int, budget_s: float, seed: int):
+    """Reference generated OpenMP C (oracle/_ref), all host threads, on the same workload."""
+    from oracle import ref
+
+    if not ref.available("sinh3d"):
+        return None
+    m1, z1, m2, z2 = bl_params(seed)
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    rg = ref.RefGrid("sinh3d", NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2)
+    for _ in range(max(1, min(warmup, 1))):
+        rg.step(1)
+    t0 = time.perf_counter()
+    rg.step(1)
+    t1 = time.perf_counter() - t0
+    n = max(1, min(steps_wanted, int(budget_s / max(t1, 1e-9))))
+    t0 = time.perf_counter()
+    rg.step(n)
+    dt = time.perf_counter() - t0
+    rg.close()
+    pts = NXX[0] * NXX[1] * NXX[2]
+    return {"value": pts * n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
+            "kind": "reference",
+            "sample": f"{n} RK4 steps of the full 256x64x64 SinhSpherical grid (reference generated OpenMP C, "
+                      f"MoL_step_forward_in_time incl. BCs + detgammabar), after 1 warm-up step",
+            "s_per_step": dt / n}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    budget = 150.0
+    res = cpu_reference_rate(args.steps, args.warmup, budget, args.seed)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/sinh3d not built (run oracle/gen_ref.py)"}))
+        return
+    line = {
+        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["s_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (Brill-Lindquist initial data, seeded)",
+        "config": {"workload": "BSSN RK4, SinhSpherical 256x64x64 (+3 ghosts), AMPL=10, SINHW=0.2, KO, radiation BCs"},
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", type=int, default=1, help="0: reference stage order; 1: fused stages")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+
+    from nrpy_b200 import lib as L
+    from nrpy_b200.grid import BSSNGrid
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    lib = L.load()
+    m1, z1, m2, z2 = bl_params(args.seed + rank)
+    grid = BSSNGrid(coord="SinhSpherical", Nxx=NXX, grid_physical_size=AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1,
+                    BH2_mass=m2, BH2_posn_z=z2)
+    pts = grid.n_interior
+    y0 = grid.y_n.clone()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- device-resident timed region: CUDA-graph RK4 steps + H every 20 steps
+    stream = grid.make_stepper(mode=args.mode, mixed=False, steps_per_graph=1)
+    h_hist = []
+    with torch.cuda.stream(stream):
+        grid.run_stepper(args.warmup)
+        grid.constraint_norms()
+    torch.cuda.synchronize()
+    grid.y_n.copy_(y0)
+    barrier()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = lib.bssn_b200_kernel_launches()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            done = 0
+            while done < args.steps:
+                n = min(H_EVERY, args.steps - done)
+                grid.run_stepper(n)
+                done += n
+                if done % H_EVERY == 0:
+                    h_hist.append(grid.constraint_norms()["H_L2"])
+            stop.record(stream)
+        stop.synchronize()
+    launches = lib.bssn_b200_kernel_launches() - launches0
+    ms = start.elapsed_time(stop)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * pts * args.steps / (ms * 1e-3)
+    clocks = clk.summary()
+
+    # ---------------- dominant kernel alone: fused interior RHS + RK update, per stage
+    kstats = time_fused_kernel(grid, lib, stream, reps=5)
+    peak, peak_kind = peaks()
+    bytes_launch = np.mean(STAGE_WORDS) * 8 * pts
+    achieved = bytes_launch / (kstats["ms_per_launch"] * 1e-3) / 1e9
+
+    # ---------------- end-to-end through the public API with host buffers
+    e2e = run_e2e(grid, args, y0)
+    grid.free_stepper()
+
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                cpu = cpu_reference_rate(3, 1, 25.0, args.seed)
+            except Exception as e:  # noqa: BLE001
+                cpu = {"unavailable": str(e)}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (Brill-Lindquist initial data, seeded)",
+            "config": {"workload": "BSSN RK4, SinhSpherical 256x64x64 (+3 ghosts), AMPL=10, SINHW=0.2, FP64, "
+                                   "KO, radiation BCs, H-constraint L2 every 20 steps",
+                       "interior_points": pts, "mode": "fused stages" if args.mode == 1 else "reference stage order",
+                       "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",
+                       "parallelism": f"replicas x{world}", "seed": args.seed, "bl": [m1, z1, m2, z2],
+                       "dt": grid.dt, "H_L2_last": h_hist[-1] if h_hist else None},
+            "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel (interior RHS + RK4 update + projection)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": kstats["ms_per_launch"],
+                         "step_achieved": value / world * B_ALG_PER_PT_STEP / 1e9,
+                         "step_frac": value / world * B_ALG_PER_PT_STEP / 1e9 / peak},
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    grid.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def time_fused_kernel(grid, lib, stream, reps: int = 5):
+    import torch
+
+    from nrpy_b200 import lib as L
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(4 * reps)]
+    k = 0
+    for r in range(reps):
+        for stage in (1, 2, 3, 4):
+            a, b = ev[k]
+            a.record(stream)
+            L.check(lib.bssn_b200_rhs_fused_stage(C.byref(grid.cd), grid.gd, stage, 0, C.c_void_p(stream.cuda_stream)))
+            b.record(stream)
+            k += 1
+    torch.cuda.synchronize()
+    t = [a.elapsed_time(b) for a, b in ev[4:]]  # first round is warm-up
+    return {"ms_per_launch": float(np.mean(t))}
+
+
+def run_e2e(grid, args, y0):
+    """Per step: pinned-host state -> device, one RK4 step through BSSNGrid (public API),
+    device -> pinned-host state; H-constraint L2 read back every 20 steps."""
+    import torch
+
+    host_in = y0.cpu().pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    steps = min(args.steps, 50)
+    cur = torch.cuda.current_stream()
+    for _ in range(3):
+        grid.y_n.copy_(host_in, non_blocking=True)
+        grid.MoL_step_forward_in_time(mode=args.mode)
+        host_out.copy_(grid.y_n, non_blocking=True)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(cur)
+    for s in range(steps):
+        grid.y_n.copy_(host_in, non_blocking=True)
+        grid.MoL_step_forward_in_time(mode=args.mode)
+        host_out.copy_(grid.y_n, non_blocking=True)
+        if (s + 1) % H_EVERY == 0:
+            grid.constraint_norms()
+    b.record(cur)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    nbytes = grid.y_n.numel() * 8
+    return {"value": grid.n_interior * steps / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes, "steps": steps}
+
+
+if __name__ == "__main__":
+    main()

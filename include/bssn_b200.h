@@ -1,0 +1,317 @@
+/*
+ * bssn_b200.h -- C ABI of libbssn_b200.so, a B200 (sm_100a) implementation of the
+ * BlackHoles@Home single-patch BSSN evolution step.
+ *
+ * The struct layouts and the void entry points are those of the C project that NRPy's
+ * BHaH generator emits for a BSSN evolution (two_blackholes_collide-style, Kreiss-Oliger
+ * on, CodeParameters of both Spherical and SinhSpherical registered), so a caller of
+ * that project's step functions can link this library instead. Each entry point cites
+ * the generator of the function it replaces (paths relative to the nrpy repository).
+ *
+ * Memory convention (the reference's CUDA build keeps the same split):
+ *   - gridfunction arrays (in_gfs, rhs_gfs, auxevol_gfs, y_n_gfs, ..., diagnostic_gfs)
+ *     and xx[3] are DEVICE arrays, laid out IDX4(gf,i0,i1,i2) = i0 + N0*(i1 + N1*(i2 + N2*gf));
+ *   - params_struct / commondata_struct are HOST structs;
+ *   - rfm_struct and bc_struct are HOST structs whose array members point to DEVICE memory
+ *     (filled by rfm_precompute_defines() and bcstruct_set_up() of this library).
+ * The void entry points launch on the legacy default stream and return when the work
+ * is queued; fatal errors print to stderr and exit(1), as the reference does. The
+ * bssn_b200_* entry points take an explicit stream and return 0 or a negative status,
+ * with the message available from bssn_b200_last_error().
+ */
+#ifndef BSSN_B200_H
+#define BSSN_B200_H
+
+#include <stdbool.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <time.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef REAL
+#define REAL double
+#endif
+#define NGHOSTS 3
+#define NUM_EVOL_GFS 24
+#define NUM_AUXEVOL_GFS 6
+#define MAXNUMGRIDS 15
+
+/* Evolved gridfunction indices (BHaH_defines.h "EVOL VARIABLES"). */
+enum {
+  ADD00GF, ADD01GF, ADD02GF, ADD11GF, ADD12GF, ADD22GF, ALPHAGF, BETU0GF, BETU1GF, BETU2GF,
+  CFGF, HDD00GF, HDD01GF, HDD02GF, HDD11GF, HDD12GF, HDD22GF, LAMBDAU0GF, LAMBDAU1GF,
+  LAMBDAU2GF, TRKGF, VETU0GF, VETU1GF, VETU2GF
+};
+/* Auxiliary evolution gridfunctions: the conformal Ricci tensor. */
+enum { RBARDD00GF, RBARDD01GF, RBARDD02GF, RBARDD11GF, RBARDD12GF, RBARDD22GF };
+/* Diagnostic gridfunctions written by constraints_eval() (a 3-slot array). */
+enum { BSSN_B200_DIAG_HAMILTONIAN, BSSN_B200_DIAG_MSQUARED, BSSN_B200_DIAG_LAMBDA_CONSTRAINT, BSSN_B200_NUM_DIAG_GFS };
+
+/* CoordSystem_hash values (BHaH_defines.h). */
+#define SPHERICAL 1307621703
+#define SINHSPHERICAL 579707936
+
+/* commondata_struct: CodeParameters shared by all grids (BHaH_defines_h.py, CodeParameters.py:17-199). */
+typedef struct __commondata_struct__ {
+  REAL BH1_mass;
+  REAL BH1_posn_x;
+  REAL BH1_posn_y;
+  REAL BH1_posn_z;
+  REAL BH2_mass;
+  REAL BH2_posn_x;
+  REAL BH2_posn_y;
+  REAL BH2_posn_z;
+  REAL CFL_FACTOR;
+  REAL KreissOliger_strength_gauge;
+  REAL KreissOliger_strength_nongauge;
+  REAL convergence_factor;
+  REAL diagnostics_output_every;
+  REAL dt;
+  REAL eta;
+  REAL t_0;
+  REAL t_final;
+  REAL time;
+  struct timespec start_wallclock_time;
+  char outer_bc_type[50];
+  int NUMGRIDS;
+  int nn;
+  int nn_0;
+  int output_progress_every;
+} commondata_struct;
+
+/* params_struct: per-grid CodeParameters (BHaH_defines_h.py; numerical_grids_and_timestep.py). */
+typedef struct __params_struct__ {
+  REAL AMPL;
+  REAL Cart_originx;
+  REAL Cart_originy;
+  REAL Cart_originz;
+  REAL PI;
+  REAL RMAX;
+  REAL SINHW;
+  REAL dxx0;
+  REAL dxx1;
+  REAL dxx2;
+  REAL grid_hole_radius;
+  REAL grid_physical_size;
+  REAL invdxx0;
+  REAL invdxx1;
+  REAL invdxx2;
+  REAL xmax;
+  REAL xmin;
+  REAL xxmax0;
+  REAL xxmax1;
+  REAL xxmax2;
+  REAL xxmin0;
+  REAL xxmin1;
+  REAL xxmin2;
+  REAL ymax;
+  REAL ymin;
+  REAL zmax;
+  REAL zmin;
+  bool grid_rotates;
+  bool is_host;
+  char CoordSystemName[100];
+  char gridname[100];
+  int CoordSystem_hash;
+  int Nxx0;
+  int Nxx1;
+  int Nxx2;
+  int Nxx_plus_2NGHOSTS0;
+  int Nxx_plus_2NGHOSTS1;
+  int Nxx_plus_2NGHOSTS2;
+  int grid_idx;
+} params_struct;
+
+/* rfm_struct: 1-D reference-metric precompute arrays (rfm_precompute.py:84-565). The
+ * SinhSpherical field list is used for both coordinate systems; for Spherical the radial
+ * derivatives are 1, 0, 0. Array members are device pointers. */
+typedef struct __rfmstruct__ {
+  REAL *f0_of_xx0;
+  REAL *f0_of_xx0__D0;
+  REAL *f0_of_xx0__DD00;
+  REAL *f0_of_xx0__DDD000;
+  REAL *f1_of_xx1;
+  REAL *f1_of_xx1__D1;
+  REAL *f1_of_xx1__DD11;
+} rfm_struct;
+
+/* Curvilinear boundary-condition structures (CurviBoundaryConditions/BHaH_defines.py:41-199). */
+typedef struct __innerpt_bc_struct__ {
+  int dstpt;
+  int srcpt;
+  int8_t parity[10];
+} innerpt_bc_struct;
+
+typedef struct __outerpt_bc_struct__ {
+  short i0, i1, i2;
+  int8_t FACEX0, FACEX1, FACEX2;
+} outerpt_bc_struct;
+
+typedef struct __bc_info_struct__ {
+  int num_inner_boundary_points;
+  int num_pure_outer_boundary_points[NGHOSTS][3];
+  int bc_loop_bounds[NGHOSTS][6][6];
+} bc_info_struct;
+
+typedef struct __bc_struct__ {
+  innerpt_bc_struct *inner_bc_array;               /* device */
+  outerpt_bc_struct *pure_outer_bc_array[NGHOSTS * 3]; /* device */
+  bc_info_struct bc_info;
+} bc_struct;
+
+/* Method-of-lines RK4 storage (MoLtimestepping/BHaH_defines.py:18). Device arrays. */
+typedef struct __MoL_gridfunctions_struct__ {
+  REAL *y_n_gfs;
+  REAL *y_nplus1_running_total_gfs;
+  REAL *k_odd_gfs;
+  REAL *k_even_gfs;
+  REAL *auxevol_gfs;
+} MoL_gridfunctions_struct;
+
+typedef struct __griddata__ {
+  REAL *xx[3]; /* device */
+  bc_struct bcstruct;
+  MoL_gridfunctions_struct gridfuncs;
+  params_struct params;
+  rfm_struct *rfmstruct; /* host struct, device arrays */
+} griddata_struct;
+
+/* Per-gridfunction parity type, outer-boundary wave speed and asymptotic value
+ * (BHaH_defines.h: evol_gf_parity, gridfunctions_wavespeed, gridfunctions_f_infinity). */
+extern const int8_t bssn_b200_evol_gf_parity[NUM_EVOL_GFS];
+extern const REAL gridfunctions_wavespeed[NUM_EVOL_GFS];
+extern const REAL gridfunctions_f_infinity[NUM_EVOL_GFS];
+
+/* ======================= drop-in entry points (void, exit(1) on error) ======================= */
+
+/* Defaults of every CodeParameter (CodeParameters.py: params/commondata_struct_set_to_default). */
+void commondata_struct_set_to_default(commondata_struct *commondata);
+void params_struct_set_to_default(commondata_struct *commondata, griddata_struct *griddata);
+
+/* numerical_grids_and_timestep.py:31-190 -- Nxx, dxx, invdxx, cell-centred xx[3] (allocated on device). */
+void numerical_grid_params_Nxx_dxx_xx(const commondata_struct *commondata, params_struct *params, REAL *xx[3],
+                                      const int Nx[3], const bool apply_convergence_factor_and_set_xxminmax_defaults);
+/* rfm_precompute.py:84-565 */
+void rfm_precompute_malloc(const commondata_struct *commondata, const params_struct *params, rfm_struct *rfmstruct);
+void rfm_precompute_defines(const commondata_struct *commondata, const params_struct *params, rfm_struct *rfmstruct,
+                            REAL *xx[3]);
+void rfm_precompute_free(const commondata_struct *commondata, const params_struct *params, rfm_struct *rfmstruct);
+/* CurviBoundaryConditions/bcstruct_set_up.py:442-792 (computed on the host, arrays uploaded). */
+void bcstruct_set_up(const commondata_struct *commondata, const params_struct *params, REAL *xx[3], bc_struct *bcstruct);
+void bcstruct_free(bc_struct *bcstruct);
+/* numerical_grids_and_timestep.py:498-560 -- dt = min(dt, CFL_FACTOR * min ds). */
+void cfl_limited_timestep(commondata_struct *commondata, params_struct *params, REAL *xx[3]);
+/* general_relativity/initial_data.py:24 with Brill-Lindquist data (InitialData_Cartesian.py:111-141) and the
+ * ADM->BSSN converter (ADM_Initial_Data_Reader__BSSN_Converter.py:33-1181). Needs y_n_gfs allocated. */
+void initial_data(commondata_struct *commondata, griddata_struct *griddata);
+/* MoLtimestepping/register_all.py */
+void MoL_malloc_y_n_gfs(const commondata_struct *commondata, const params_struct *params, MoL_gridfunctions_struct *gridfuncs);
+void MoL_malloc_intermediate_stage_gfs(const commondata_struct *commondata, const params_struct *params,
+                                       MoL_gridfunctions_struct *gridfuncs);
+void MoL_free_intermediate_stage_gfs(MoL_gridfunctions_struct *gridfuncs);
+
+/* general_relativity/Ricci_eval.py:27-167 */
+void Ricci_eval(const params_struct *params, const rfm_struct *rfmstruct, const REAL *in_gfs, REAL *auxevol_gfs);
+/* general_relativity/rhs_eval.py:38-413 */
+void rhs_eval(const commondata_struct *commondata, const params_struct *params, const rfm_struct *rfmstruct,
+              const REAL *auxevol_gfs, const REAL *in_gfs, REAL *rhs_gfs);
+/* CurviBoundaryConditions/apply_bcs_outerradiation_and_inner.py:46-723 */
+void apply_bcs_outerradiation_and_inner(const commondata_struct *commondata, const params_struct *params,
+                                        const bc_struct *bcstruct, REAL *xx[3], const REAL custom_wavespeed[NUM_EVOL_GFS],
+                                        const REAL custom_f_infinity[NUM_EVOL_GFS], REAL *gfs, REAL *rhs_gfs);
+/* CurviBoundaryConditions/apply_bcs_outerextrap_and_inner.py:28-398 */
+void apply_bcs_outerextrap_and_inner(const commondata_struct *commondata, const params_struct *params,
+                                     const bc_struct *bcstruct, REAL *gfs);
+/* CurviBoundaryConditions/apply_bcs_inner_only.py:26-199 */
+void apply_bcs_inner_only(const commondata_struct *commondata, const params_struct *params, const bc_struct *bcstruct,
+                          REAL *gfs);
+/* general_relativity/enforce_detgammabar_equals_detgammahat.py:198-342 */
+void enforce_detgammabar_equals_detgammahat(const params_struct *params, const rfm_struct *rfmstruct, REAL *in_gfs,
+                                            const REAL *auxevol_gfs);
+/* MoLtimestepping/MoL_step_forward_in_time.py:39-507 (RK4, radiation or extrapolation outer BCs). */
+void MoL_step_forward_in_time(commondata_struct *commondata, griddata_struct *griddata);
+/* general_relativity/constraints_eval.py:364-492 -- diagnostic_gfs holds BSSN_B200_NUM_DIAG_GFS gridfunctions
+ * (H, M^2, |Lambda constraint|) on the device; interior points are written. */
+void constraints_eval(const commondata_struct *commondata, const params_struct *params, const rfm_struct *rfmstruct,
+                      const REAL *in_gfs, const REAL *auxevol_gfs, REAL *diagnostic_gfs);
+
+/* ======================= status-returning entry points (explicit stream) ======================= */
+/* `stream` is a cudaStream_t passed as void* (NULL = legacy default stream). Return 0 on success,
+ * a negative BSSN_B200_E* code otherwise; bssn_b200_last_error() describes the last failure. */
+enum {
+  BSSN_B200_OK = 0,
+  BSSN_B200_EINVAL = -1,   /* bad argument (size, pointer, coordinate system, symmetry) */
+  BSSN_B200_ECUDA = -2,    /* a CUDA runtime call or kernel launch failed */
+  BSSN_B200_ESETUP = -3,   /* boundary set-up failed (a ghost point did not map to the grid) */
+  BSSN_B200_ENOMEM = -4
+};
+const char *bssn_b200_last_error(void);
+const char *bssn_b200_version(void);
+
+/* Symmetry axes of the generated algebra: "" (full 3-D, default) or "2" (axisymmetric:
+ * derivatives in xx2 vanish, as nrpy's symmetry_axes="2"). Process-wide setting. */
+int bssn_b200_set_symmetry_axes(const char *axes);
+
+int bssn_b200_ricci_eval(const params_struct *params, const rfm_struct *rfmstruct, const REAL *in_gfs,
+                         REAL *auxevol_gfs, void *stream);
+int bssn_b200_rhs_eval(const commondata_struct *commondata, const params_struct *params, const rfm_struct *rfmstruct,
+                       const REAL *auxevol_gfs, const REAL *in_gfs, REAL *rhs_gfs, void *stream);
+/* rhs_eval with the RHS algebra (not the stencils) in FP32; state and outputs stay FP64. */
+int bssn_b200_rhs_eval_mixed(const commondata_struct *commondata, const params_struct *params,
+                             const rfm_struct *rfmstruct, const REAL *auxevol_gfs, const REAL *in_gfs, REAL *rhs_gfs,
+                             void *stream);
+int bssn_b200_apply_bcs_outerradiation_and_inner(const commondata_struct *commondata, const params_struct *params,
+                                                 const bc_struct *bcstruct, REAL *xx[3], const REAL *wavespeed,
+                                                 const REAL *f_infinity, REAL *gfs, REAL *rhs_gfs, void *stream);
+int bssn_b200_apply_bcs_outerextrap_and_inner(const params_struct *params, const bc_struct *bcstruct, REAL *gfs,
+                                              void *stream);
+int bssn_b200_apply_bcs_inner_only(const params_struct *params, const bc_struct *bcstruct, REAL *gfs, int num_gfs,
+                                   const int8_t *gf_parity_types, void *stream);
+int bssn_b200_enforce_detgammabar_equals_detgammahat(const params_struct *params, const rfm_struct *rfmstruct,
+                                                     REAL *in_gfs, void *stream);
+int bssn_b200_constraints_eval(const commondata_struct *commondata, const params_struct *params,
+                               const rfm_struct *rfmstruct, const REAL *in_gfs, const REAL *auxevol_gfs,
+                               REAL *diagnostic_gfs, void *stream);
+/* Volume integrals over the interior (diagnostics_volume_integration_helpers.h:400-470):
+ * out[0..2] = sum_interior f^2 dV for f = H, M^2, |Lambda|; out[3] = sum dV, with
+ * dV = sqrt(det gammahat) |dxx0 dxx1 dxx2|. `out` is a HOST array, written after the
+ * stream synchronises. The L2 norm of f is sqrt(out[k]); its RMS is sqrt(out[k]/out[3]).
+ * Uses a device scratch buffer that the library allocates on first use and keeps. */
+int bssn_b200_constraint_integrals(const params_struct *params, const rfm_struct *rfmstruct,
+                                   const REAL *diagnostic_gfs, double out[4], void *stream);
+
+/* One RK4 step (all four stages) on one grid. mode: 0 = stage-by-stage as the reference
+ * (Ricci, RHS, BCs, RK update, enforce); 1 = fused stages (RK update and detgammabar
+ * enforcement in the RHS epilogue). mixed != 0 evaluates the RHS algebra in FP32. */
+int bssn_b200_mol_step(commondata_struct *commondata, griddata_struct *griddata, int mode, int mixed, void *stream);
+
+/* A captured CUDA graph of `steps_per_graph` RK4 steps of one grid; replayed by
+ * bssn_b200_stepper_run. The graph bakes in dt and the buffer addresses. */
+typedef struct bssn_b200_stepper bssn_b200_stepper;
+int bssn_b200_stepper_create(commondata_struct *commondata, griddata_struct *griddata, int mode, int mixed,
+                             int steps_per_graph, void *stream, bssn_b200_stepper **out);
+int bssn_b200_stepper_run(bssn_b200_stepper *st, int graph_launches);
+int bssn_b200_stepper_destroy(bssn_b200_stepper *st);
+/* Number of kernel nodes in one replay of the stepper's graph. */
+int bssn_b200_stepper_kernel_nodes(const bssn_b200_stepper *st, unsigned long long *out);
+
+/* Instrumentation: kernels launched by this library since it was loaded (each graph replay
+ * counts its kernel nodes), and a launch of only the interior RHS + RK-update + projection
+ * kernel of RK4 stage `stage` (1..4) of grid 0, used to time the dominant kernel alone.
+ * The latter overwrites that stage's output buffer. */
+unsigned long long bssn_b200_kernel_launches(void);
+int bssn_b200_rhs_fused_stage(commondata_struct *commondata, griddata_struct *griddata, int stage, int mixed,
+                              void *stream);
+
+/* Synchronous copy for callers without their own CUDA binding:
+ * kind 0 = host->device, 1 = device->host, 2 = device->device. */
+int bssn_b200_memcpy(void *dst, const void *src, size_t bytes, int kind);
+int bssn_b200_device_synchronize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BSSN_B200_H */

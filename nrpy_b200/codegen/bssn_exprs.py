@@ -151,3 +151,24 @@ def enforce_exprs(coord: str) -> Dict[str, sp.Expr]:
                 (rfm.ghatDD[i][j] / rfm.ReDD[i][j]) + Bq.hDD[i][j]
             ) - (rfm.ghatDD[i][j] / rfm.ReDD[i][j])
     return out
+
+
+def lambda_id_exprs(coord: str) -> Dict[str, sp.Expr]:
+    """lambda^i = Lambdabar^i / ReU[i], Lambdabar^i = gammabar^jk (Gammabar^i_jk - Gammahat^i_jk).
+
+    ADM_Initial_Data_Reader__BSSN_Converter.py:462-580 (the reference evaluates it with the
+    closed-form reference metric; here the rfm-precompute form of the same quantities).
+    """
+    import nrpy.reference_metric as refmetric
+    from nrpy.equations.general_relativity.BSSN_quantities import BSSN_quantities
+
+    Bq = BSSN_quantities[coord + "_rfm_precompute"]
+    rfm = refmetric.reference_metric[coord + "_rfm_precompute"]
+    out = {}
+    for i in range(3):
+        lam = sp.sympify(0)
+        for j in range(3):
+            for k in range(3):
+                lam += Bq.gammabarUU[j][k] * (Bq.GammabarUDD[i][j][k] - rfm.GammahatUDD[i][j][k])
+        out[f"lambdaU{i}"] = lam / rfm.ReU[i]
+    return out

@@ -175,33 +175,38 @@ class PointKernel:
         self.lines.append(self._deriv_code(name, gf, kind, dirs))
 
     def _deriv_code(self, name: str, gf: str, kind: str, dirs: Tuple[int, ...]) -> str:
-        P = self.printer
+        """Finite-difference statement, evaluated in the stencil type TF, stored as T."""
+
+        def c(r) -> str:  # rational constant in TF
+            p, q = int(sp.Rational(r).p), int(sp.Rational(r).q)
+            return f"TF({p}.0/{q}.0)" if q != 1 else f"TF({p}.0)"
+
+        def v(var: str) -> str:
+            return f"TF({var})"
+
         if kind == "D":
             (d,) = dirs
             w = fdc.first_centred()
-            terms = []
-            for o in sorted(k for k in w if k > 0):
-                terms.append(f"{P._print(w[o])}*(T({self._pt(gf, d, o)}) - T({self._pt(gf, d, -o)}))")
-            return f"const T {name} = T(invdxx{d}) * ({' + '.join(terms)});"
+            terms = [f"{c(w[o])}*({v(self._pt(gf, d, o))} - {v(self._pt(gf, d, -o))})" for o in sorted(k for k in w if k > 0)]
+            return f"const T {name} = T(TF(invdxx{d}) * ({' + '.join(terms)}));"
         if kind == "DD":
             d1, d2 = dirs
             if d1 == d2:
                 w = fdc.second_centred()
-                terms = [f"{P._print(w[0])}*T({self._pt(gf, d1, 0)})"]
+                terms = [f"{c(w[0])}*{v(self._pt(gf, d1, 0))}"]
                 for o in sorted(k for k in w if k > 0):
-                    terms.append(f"{P._print(w[o])}*(T({self._pt(gf, d1, o)}) + T({self._pt(gf, d1, -o)}))")
-                return f"const T {name} = T(invdxx{d1})*T(invdxx{d1}) * ({' + '.join(terms)});"
+                    terms.append(f"{c(w[o])}*({v(self._pt(gf, d1, o))} + {v(self._pt(gf, d1, -o))})")
+                return f"const T {name} = T(TF(invdxx{d1})*TF(invdxx{d1}) * ({' + '.join(terms)}));"
             w = fdc.first_centred()
             pos = sorted(k for k in w if k > 0)
 
             def inner(a: int) -> str:
                 return " + ".join(
-                    f"{P._print(w[b])}*(T({self._pt(gf, d1, a, d2, b)}) - T({self._pt(gf, d1, a, d2, -b)}))"
-                    for b in pos
+                    f"{c(w[b])}*({v(self._pt(gf, d1, a, d2, b))} - {v(self._pt(gf, d1, a, d2, -b))})" for b in pos
                 )
 
-            outer = " + ".join(f"{P._print(w[a])}*(({inner(a)}) - ({inner(-a)}))" for a in pos)
-            return f"const T {name} = T(invdxx{d1})*T(invdxx{d2}) * ({outer});"
+            outer = " + ".join(f"{c(w[a])}*(({inner(a)}) - ({inner(-a)}))" for a in pos)
+            return f"const T {name} = T(TF(invdxx{d1})*TF(invdxx{d2}) * ({outer}));"
         if kind == "upD":
             (d,) = dirs
             up = fdc.upwind(+1)
@@ -210,15 +215,15 @@ class PointKernel:
             for t in sorted(up):
                 fu = self._pt(gf, d, t)
                 fd = self._pt(gf, d, -t)
-                terms.append(f"{P._print(up[t])}*(Upwind{d} ? T({fu}) : -T({fd}))")
-            return f"const T {name} = T(invdxx{d}) * ({' + '.join(terms)});"
+                terms.append(f"{c(up[t])}*(Upwind{d} ? {v(fu)} : -{v(fd)})")
+            return f"const T {name} = T(TF(invdxx{d}) * ({' + '.join(terms)}));"
         if kind == "KOD":
             (d,) = dirs
             w = fdc.kreiss_oliger()
-            terms = [f"{P._print(w[0])}*T({self._pt(gf, d, 0)})"]
+            terms = [f"{c(w[0])}*{v(self._pt(gf, d, 0))}"]
             for o in sorted(k for k in w if k > 0):
-                terms.append(f"{P._print(w[o])}*(T({self._pt(gf, d, o)}) + T({self._pt(gf, d, -o)}))")
-            return f"const T {name} = T(invdxx{d}) * ({' + '.join(terms)});"
+                terms.append(f"{c(w[o])}*({v(self._pt(gf, d, o))} + {v(self._pt(gf, d, -o))})")
+            return f"const T {name} = T(TF(invdxx{d}) * ({' + '.join(terms)}));"
         raise ValueError(kind)
 
     def _ensure(self, expr: sp.Expr) -> None:
@@ -264,7 +269,7 @@ def emit_point_function(
     body = pk.build(outputs, upwind_vec)
     head = f"// {comment}\n" if comment else ""
     code = (
-        f"{head}template <typename T, typename Ctx>\n"
+        f"{head}template <typename T, typename TF, typename Ctx>\n"
         f"__device__ __forceinline__ void {fname}(const Ctx &ctx, T *__restrict__ out) {{\n"
         f"{body}\n}}\n"
     )

@@ -73,6 +73,16 @@ def generate_variant(tag: str) -> None:
     )
     parts.append(code)
     stats["enforce"] = st
+    lam = be.lambda_id_exprs(coord)
+    code, st = emit_point_function(
+        f"lambda_point_{tag}",
+        [(f"out[{i}]", lam[f"lambdaU{i}"]) for i in range(3)],
+        symmetry_axes=sym,
+        comment=f"initial-data lambda^i from centred FD of hDD, {coord}: "
+        "ADM_Initial_Data_Reader__BSSN_Converter.py:462-580",
+    )
+    parts.append(code)
+    stats["lambda"] = st
     hdr = (
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', 4th-order FD, KO (CAKO).\n"

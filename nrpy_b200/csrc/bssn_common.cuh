@@ -1,0 +1,130 @@
+// Internal definitions shared by the libbssn_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "bssn_b200.h"
+
+namespace bssn {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char *fmt, ...);
+const char *last_error();
+void count_launch(unsigned long long n);
+
+#define BSSN_CUDA_TRY(call)                                                                                  \
+  do {                                                                                                       \
+    cudaError_t err_ = (call);                                                                               \
+    if (err_ != cudaSuccess) {                                                                               \
+      ::bssn::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(err_));                \
+      return BSSN_B200_ECUDA;                                                                                \
+    }                                                                                                        \
+  } while (0)
+
+// Every kernel launch site is followed by this check; it also counts the launch.
+#define BSSN_LAUNCH_CHECK()                                                                                  \
+  do {                                                                                                       \
+    cudaError_t err_ = cudaGetLastError();                                                                   \
+    if (err_ != cudaSuccess) {                                                                               \
+      ::bssn::set_error("%s:%d: kernel launch: %s", __FILE__, __LINE__, cudaGetErrorString(err_));            \
+      return BSSN_B200_ECUDA;                                                                                \
+    }                                                                                                        \
+    ::bssn::count_launch(1);                                                                                 \
+  } while (0)
+
+#define BSSN_TRY(call)                                                                                       \
+  do {                                                                                                       \
+    int rc_ = (call);                                                                                        \
+    if (rc_ != BSSN_B200_OK) return rc_;                                                                     \
+  } while (0)
+
+// ---------------------------------------------------------------- variants
+// Generated algebra variants: CoordSystem x symmetry axes.
+enum Variant { SPH_3D = 0, SPH_AXI = 1, SINH_3D = 2, SINH_AXI = 3, NUM_VARIANTS = 4 };
+int symmetry_axes_mask();  // bit d set: derivatives in direction d vanish
+int variant_of(const params_struct *params, Variant *out);
+
+// ---------------------------------------------------------------- grid geometry passed to kernels
+struct GridDims {
+  int N0, N1, N2;      // Nxx_plus_2NGHOSTS*
+  int s1, s2;          // strides of i1, i2
+  int ntot;            // points per gridfunction
+  double invdxx0, invdxx1, invdxx2;
+};
+inline GridDims grid_dims(const params_struct *p) {
+  GridDims g;
+  g.N0 = p->Nxx_plus_2NGHOSTS0;
+  g.N1 = p->Nxx_plus_2NGHOSTS1;
+  g.N2 = p->Nxx_plus_2NGHOSTS2;
+  g.s1 = g.N0;
+  g.s2 = g.N0 * g.N1;
+  g.ntot = g.N0 * g.N1 * g.N2;
+  g.invdxx0 = p->invdxx0;
+  g.invdxx1 = p->invdxx1;
+  g.invdxx2 = p->invdxx2;
+  return g;
+}
+
+struct RfmArrays {
+  const double *f0, *f0_D0, *f0_DD00, *f0_DDD000, *f1, *f1_D1, *f1_DD11;
+};
+inline RfmArrays rfm_arrays(const rfm_struct *r) {
+  return RfmArrays{r->f0_of_xx0, r->f0_of_xx0__D0, r->f0_of_xx0__DD00, r->f0_of_xx0__DDD000,
+                   r->f1_of_xx1, r->f1_of_xx1__D1, r->f1_of_xx1__DD11};
+}
+
+struct PhysParams {
+  double eta, ko_gauge, ko_nongauge;
+};
+
+// Pointwise operators implemented in pointwise.cu.
+int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s);
+int launch_rhs(Variant v, bool mixed, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
+               const double *aux, const double *in, double *rhs, cudaStream_t s);
+int launch_constraints(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, const double *aux,
+                       double *diag, cudaStream_t s);
+int launch_enforce(Variant v, const GridDims &g, const RfmArrays &rfm, double *gfs, cudaStream_t s);
+int launch_lambda_id(Variant v, const GridDims &g, const RfmArrays &rfm, double *gfs, cudaStream_t s);
+
+// RK4 stage coefficients of the low-storage form used by the reference
+// (MoLtimestepping/MoL_step_forward_in_time.py:322-485): per stage s,
+//   s=1: run  = dt/6 K;        OUT = y + dt/2 K   (OUT = K buffer)
+//   s=2: run += dt/3 K;        OUT = y + dt/2 K
+//   s=3: run += dt/3 K;        OUT = y + dt K
+//   s=4: y    = y + run + dt/6 K
+struct StageBuffers {
+  double *y;     // y_n_gfs
+  double *run;   // y_nplus1_running_total_gfs
+  double *kin;   // stage input
+  double *kout;  // RHS / stage output buffer
+};
+int launch_rhs_fused_stage(Variant v, bool mixed, int stage, double dt, const GridDims &g, const RfmArrays &rfm,
+                           const PhysParams &pp, const double *aux, const StageBuffers &b, double *krhs,
+                           cudaStream_t s);
+int launch_rk_points(Variant v, int stage, double dt, const GridDims &g, const RfmArrays &rfm, const StageBuffers &b,
+                     const outerpt_bc_struct *pts, int npts, const double *krhs, cudaStream_t s);
+int launch_rk_substep(int stage, double dt, const GridDims &g, const StageBuffers &b, cudaStream_t s);
+
+// Boundary conditions implemented in boundary.cu.
+int launch_inner_bcs(const GridDims &g, const bc_struct *bc, double *gfs, int num_gfs, const int8_t *parity_types,
+                     cudaStream_t s);
+int launch_radiation_bcs(const GridDims &g, const params_struct *p, const bc_struct *bc, const double *const xx[3],
+                         const double *wavespeed, const double *f_inf, const double *gfs, double *rhs,
+                         cudaStream_t s);
+int launch_extrap_bcs(const GridDims &g, const bc_struct *bc, double *gfs, cudaStream_t s);
+// Fused-stage boundary update: radiation RHS at pure outer points followed by the RK update
+// of those points and the detgammabar projection; then parity copies of every inner point.
+int launch_radiation_rk_bcs(Variant v, const GridDims &g, const params_struct *p, const bc_struct *bc,
+                            const double *const xx[3], const RfmArrays &rfm, int stage, double dt,
+                            const StageBuffers &b, double *krhs_scratch, cudaStream_t s);
+
+// Device constants (wave speeds, asymptotic values, parity types).
+extern const int8_t kEvolParity[NUM_EVOL_GFS];
+extern const double kWavespeed[NUM_EVOL_GFS];
+extern const double kFInfinity[NUM_EVOL_GFS];
+
+}  // namespace bssn

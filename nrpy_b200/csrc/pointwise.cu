@@ -1,0 +1,369 @@
+// Pointwise BSSN operators: conformal Ricci tensor, RHS (upwinded advection, KO
+// dissipation), constraints, the detgammabar projection and the initial-data lambda^i.
+// The algebra is the generated code in gen/*.cuh; this file supplies the stencil-load
+// contexts and the launch geometry.
+//
+// Layout: gf-major IDX4(gf,i0,i1,i2) = i0 + N0*(i1 + N1*(i2 + N2*gf)). One thread per
+// interior point; a warp spans 32 consecutive i0, so each stencil load of a warp touches
+// one or two contiguous 256-byte segments that neighbouring warps reuse from L1/L2.
+#include "bssn_common.cuh"
+
+namespace bssn {
+
+template <typename T>
+__device__ __forceinline__ T ipow(T x, int n) {
+  T r = x;
+  for (int k = 1; k < n; k++) r *= x;
+  return r;
+}
+
+// Stencil loads from global memory around one point.
+struct PointCtx {
+  const double *__restrict__ in;   // in_gfs + IDX3(i0,i1,i2)
+  const double *__restrict__ aux;  // auxevol_gfs + IDX3(i0,i1,i2)
+  int s1, s2, ntot;
+  int i0, i1;
+  double invdxx0, invdxx1, invdxx2;
+  RfmArrays rfm;
+  double eta, KreissOliger_strength_gauge, KreissOliger_strength_nongauge;
+  __device__ __forceinline__ double ld(int gf, int a, int b, int c) const {
+    return __ldg(in + (gf * ntot + (a + b * s1 + c * s2)));
+  }
+  __device__ __forceinline__ double ldaux(int k) const { return __ldg(aux + k * ntot); }
+};
+
+// Point values held in registers (pointwise operators without stencils).
+struct RegCtx {
+  const double *v;  // NUM_EVOL_GFS values of this point
+  int i0, i1;
+  RfmArrays rfm;
+  __device__ __forceinline__ double ld(int gf, int, int, int) const { return v[gf]; }
+};
+
+#define LD(gf, a, b, c) ctx.ld(gf, a, b, c)
+#define LDAUX(k) ctx.ldaux(k)
+#define RFM(arr, d) __ldg(ctx.rfm.arr + ctx.i##d)
+#define rfm_f0 f0
+#define rfm_f0_D0 f0_D0
+#define rfm_f0_DD00 f0_DD00
+#define rfm_f0_DDD000 f0_DDD000
+#define rfm_f1 f1
+#define rfm_f1_D1 f1_D1
+#define rfm_f1_DD11 f1_DD11
+#define PARAM(name) ctx.name
+#define invdxx0 ctx.invdxx0
+#define invdxx1 ctx.invdxx1
+#define invdxx2 ctx.invdxx2
+#include "gen/bssn_sinh_3d.cuh"
+#include "gen/bssn_sinh_axi.cuh"
+#include "gen/bssn_sph_3d.cuh"
+#include "gen/bssn_sph_axi.cuh"
+#undef invdxx0
+#undef invdxx1
+#undef invdxx2
+
+#define DISPATCH_POINT(NAME, V, T, TF, CTX, OUT)                            \
+  do {                                                                      \
+    if constexpr (V == SPH_3D) NAME##_sph_3d<T, TF>(CTX, OUT);              \
+    else if constexpr (V == SPH_AXI) NAME##_sph_axi<T, TF>(CTX, OUT);       \
+    else if constexpr (V == SINH_3D) NAME##_sinh_3d<T, TF>(CTX, OUT);       \
+    else NAME##_sinh_axi<T, TF>(CTX, OUT);                                  \
+  } while (0)
+
+__device__ __forceinline__ PointCtx make_ctx(const GridDims &g, const RfmArrays &rfm, const double *in,
+                                             const double *aux, int i0, int i1, int i2) {
+  PointCtx c;
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+  c.in = in + idx;
+  c.aux = aux ? aux + idx : nullptr;
+  c.s1 = g.s1;
+  c.s2 = g.s2;
+  c.ntot = g.ntot;
+  c.i0 = i0;
+  c.i1 = i1;
+  c.invdxx0 = g.invdxx0;
+  c.invdxx1 = g.invdxx1;
+  c.invdxx2 = g.invdxx2;
+  c.rfm = rfm;
+  c.eta = 0.0;
+  c.KreissOliger_strength_gauge = 0.0;
+  c.KreissOliger_strength_nongauge = 0.0;
+  return c;
+}
+
+// Interior block geometry: 32 points along i0 x 4 along i1, one i2 plane per blockIdx.z.
+constexpr int BX = 32, BY = 4;
+static dim3 interior_grid(const GridDims &g) {
+  const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
+  return dim3((n0 + BX - 1) / BX, (n1 + BY - 1) / BY, n2);
+}
+
+#define INTERIOR_INDEX_OR_RETURN(g)                       \
+  const int i0 = NGHOSTS + blockIdx.x * BX + threadIdx.x; \
+  const int i1 = NGHOSTS + blockIdx.y * BY + threadIdx.y; \
+  const int i2 = NGHOSTS + blockIdx.z;                    \
+  if (i0 >= g.N0 - NGHOSTS || i1 >= g.N1 - NGHOSTS) return;
+
+template <Variant V>
+__global__ void __launch_bounds__(BX *BY, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
+                                                       const double *__restrict__ in, double *__restrict__ aux) {
+  INTERIOR_INDEX_OR_RETURN(g);
+  const PointCtx ctx = make_ctx(g, rfm, in, nullptr, i0, i1, i2);
+  double out[6];
+  DISPATCH_POINT(ricci_point, V, double, double, ctx, out);
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+#pragma unroll
+  for (int k = 0; k < 6; k++) aux[idx + k * g.ntot] = out[k];
+}
+
+template <Variant V, typename T>
+__global__ void __launch_bounds__(BX *BY, 1) rhs_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
+                                                     const double *__restrict__ aux, const double *__restrict__ in,
+                                                     double *__restrict__ rhs) {
+  INTERIOR_INDEX_OR_RETURN(g);
+  PointCtx ctx = make_ctx(g, rfm, in, aux, i0, i1, i2);
+  ctx.eta = pp.eta;
+  ctx.KreissOliger_strength_gauge = pp.ko_gauge;
+  ctx.KreissOliger_strength_nongauge = pp.ko_nongauge;
+  T out[NUM_EVOL_GFS];
+  DISPATCH_POINT(rhs_point, V, T, double, ctx, out);
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+#pragma unroll
+  for (int k = 0; k < NUM_EVOL_GFS; k++) rhs[idx + k * g.ntot] = double(out[k]);
+}
+
+template <Variant V>
+__global__ void __launch_bounds__(BX *BY, 1) constraints_kernel(const GridDims g, const RfmArrays rfm,
+                                                             const double *__restrict__ in,
+                                                             const double *__restrict__ aux,
+                                                             double *__restrict__ diag) {
+  INTERIOR_INDEX_OR_RETURN(g);
+  const PointCtx ctx = make_ctx(g, rfm, in, aux, i0, i1, i2);
+  double out[3];
+  DISPATCH_POINT(constraints_point, V, double, double, ctx, out);
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+#pragma unroll
+  for (int k = 0; k < 3; k++) diag[idx + k * g.ntot] = out[k];
+}
+
+// lambda^i = Lambdabar^i / ReU[i] from centred derivatives of hDD (initial data;
+// ADM_Initial_Data_Reader__BSSN_Converter.py:462-580). Writes LAMBDAU0..2 of the interior.
+template <Variant V>
+__global__ void __launch_bounds__(BX *BY) lambda_id_kernel(const GridDims g, const RfmArrays rfm,
+                                                           double *__restrict__ gfs) {
+  INTERIOR_INDEX_OR_RETURN(g);
+  const PointCtx ctx = make_ctx(g, rfm, gfs, nullptr, i0, i1, i2);
+  double out[3];
+  DISPATCH_POINT(lambda_point, V, double, double, ctx, out);
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+#pragma unroll
+  for (int k = 0; k < 3; k++) gfs[idx + (LAMBDAU0GF + k) * g.ntot] = out[k];
+}
+
+// detgammabar = detgammahat projection of hDD at ALL points (ghost zones included).
+template <Variant V>
+__global__ void enforce_kernel(const GridDims g, const RfmArrays rfm, double *__restrict__ gfs) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= g.ntot) return;
+  const int i2 = idx / g.s2;
+  const int rem = idx - i2 * g.s2;
+  const int i1 = rem / g.s1;
+  const int i0 = rem - i1 * g.s1;
+  const PointCtx ctx = make_ctx(g, rfm, gfs, nullptr, i0, i1, i2);
+  double out[6];
+  DISPATCH_POINT(enforce_point, V, double, double, ctx, out);
+#pragma unroll
+  for (int k = 0; k < 6; k++) gfs[idx + (HDD00GF + k) * g.ntot] = out[k];
+}
+
+// ---------------------------------------------------------------- fused RK stage
+// Same association as the reference's rk_substep_{1..4} (MoL_step_forward_in_time.py:346-470).
+template <int STAGE>
+__device__ __forceinline__ void rk_update(const double k, const double y, double &run, double &out, const double dt) {
+  if constexpr (STAGE == 1) {
+    run = (1.0 / 6.0) * dt * k;
+    out = (1.0 / 2.0) * dt * k + y;
+  } else if constexpr (STAGE == 2) {
+    run = (1.0 / 3.0) * dt * k + run;
+    out = (1.0 / 2.0) * dt * k + y;
+  } else if constexpr (STAGE == 3) {
+    run = (1.0 / 3.0) * dt * k + run;
+    out = dt * k + y;
+  } else {
+    out = (1.0 / 6.0) * dt * k + y + run;
+  }
+}
+
+template <Variant V, int STAGE>
+__device__ __forceinline__ void rk_and_project_point(const GridDims &g, const RfmArrays &rfm, const StageBuffers &b,
+                                                     const int idx, const int i0, const int i1, const double *kk,
+                                                     const double dt) {
+  double o[NUM_EVOL_GFS];
+#pragma unroll
+  for (int k = 0; k < NUM_EVOL_GFS; k++) {
+    const size_t a = idx + (size_t)k * g.ntot;
+    double run = (STAGE == 1) ? 0.0 : b.run[a];
+    rk_update<STAGE>(kk[k], b.y[a], run, o[k], dt);
+    if (STAGE != 4) b.run[a] = run;
+  }
+  RegCtx rc{o, i0, i1, rfm};
+  double h[6];
+  DISPATCH_POINT(enforce_point, V, double, double, rc, h);
+#pragma unroll
+  for (int k = 0; k < 6; k++) o[HDD00GF + k] = h[k];
+#pragma unroll
+  for (int k = 0; k < NUM_EVOL_GFS; k++) b.kout[idx + (size_t)k * g.ntot] = o[k];
+}
+
+// RHS at an interior point, then in registers the RK4 stage update and the detgammabar
+// projection of the stage output. The raw RHS is also stored to `krhs` on the interior
+// shell (the layer next to each face), where the outer radiation condition reads it.
+template <Variant V, typename T, int STAGE>
+__global__ void __launch_bounds__(BX *BY, 1) rhs_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
+                                                           const double *__restrict__ aux, const StageBuffers b,
+                                                           double *__restrict__ krhs, const double dt) {
+  INTERIOR_INDEX_OR_RETURN(g);
+  PointCtx ctx = make_ctx(g, rfm, b.kin, aux, i0, i1, i2);
+  ctx.eta = pp.eta;
+  ctx.KreissOliger_strength_gauge = pp.ko_gauge;
+  ctx.KreissOliger_strength_nongauge = pp.ko_nongauge;
+  T kt[NUM_EVOL_GFS];
+  DISPATCH_POINT(rhs_point, V, T, double, ctx, kt);
+  double kk[NUM_EVOL_GFS];
+#pragma unroll
+  for (int k = 0; k < NUM_EVOL_GFS; k++) kk[k] = double(kt[k]);
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+  const bool shell = (i0 == NGHOSTS) | (i0 == g.N0 - NGHOSTS - 1) | (i1 == NGHOSTS) | (i1 == g.N1 - NGHOSTS - 1) |
+                     (i2 == NGHOSTS) | (i2 == g.N2 - NGHOSTS - 1);
+  if (shell) {
+#pragma unroll
+    for (int k = 0; k < NUM_EVOL_GFS; k++) krhs[idx + (size_t)k * g.ntot] = kk[k];
+  }
+  rk_and_project_point<V, STAGE>(g, rfm, b, idx, i0, i1, kk, dt);
+}
+
+// RK update plus projection of listed boundary points whose RHS is already in krhs.
+template <Variant V, int STAGE>
+__global__ void rk_points_kernel(const GridDims g, const RfmArrays rfm, const StageBuffers b,
+                                 const outerpt_bc_struct *__restrict__ pts, const int npts,
+                                 const double *__restrict__ krhs, const double dt) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  const outerpt_bc_struct p = pts[t];
+  const int idx = p.i0 + g.s1 * p.i1 + g.s2 * p.i2;
+  double kk[NUM_EVOL_GFS];
+#pragma unroll
+  for (int k = 0; k < NUM_EVOL_GFS; k++) kk[k] = krhs[idx + (size_t)k * g.ntot];
+  rk_and_project_point<V, STAGE>(g, rfm, b, idx, p.i0, p.i1, kk, dt);
+}
+
+// ---------------------------------------------------------------- launchers
+template <template <Variant> class K>
+struct Dummy {};
+
+#define VARIANT_SWITCH(v, CALL)                 \
+  switch (v) {                                  \
+    case SPH_3D: { constexpr Variant VV = SPH_3D; CALL; } break;   \
+    case SPH_AXI: { constexpr Variant VV = SPH_AXI; CALL; } break; \
+    case SINH_3D: { constexpr Variant VV = SINH_3D; CALL; } break; \
+    case SINH_AXI: { constexpr Variant VV = SINH_AXI; CALL; } break; \
+    default: set_error("unknown algebra variant %d", (int)v); return BSSN_B200_EINVAL; \
+  }
+
+static bool empty_interior(const GridDims &g) {
+  return g.N0 <= 2 * NGHOSTS || g.N1 <= 2 * NGHOSTS || g.N2 <= 2 * NGHOSTS;
+}
+
+int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
+  if (empty_interior(g)) return BSSN_B200_OK;
+  VARIANT_SWITCH(v, (ricci_kernel<VV><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, in, aux)));
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+int launch_rhs(Variant v, bool mixed, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
+               const double *aux, const double *in, double *rhs, cudaStream_t s) {
+  if (empty_interior(g)) return BSSN_B200_OK;
+  if (mixed) {
+    VARIANT_SWITCH(v, (rhs_kernel<VV, float><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, pp, aux, in, rhs)));
+  } else {
+    VARIANT_SWITCH(v, (rhs_kernel<VV, double><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, pp, aux, in, rhs)));
+  }
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+int launch_constraints(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, const double *aux,
+                       double *diag, cudaStream_t s) {
+  if (empty_interior(g)) return BSSN_B200_OK;
+  VARIANT_SWITCH(v, (constraints_kernel<VV><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, in, aux, diag)));
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+int launch_lambda_id(Variant v, const GridDims &g, const RfmArrays &rfm, double *gfs, cudaStream_t s) {
+  if (empty_interior(g)) return BSSN_B200_OK;
+  VARIANT_SWITCH(v, (lambda_id_kernel<VV><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, gfs)));
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+int launch_enforce(Variant v, const GridDims &g, const RfmArrays &rfm, double *gfs, cudaStream_t s) {
+  const int threads = 128;
+  const int blocks = (g.ntot + threads - 1) / threads;
+  VARIANT_SWITCH(v, (enforce_kernel<VV><<<blocks, threads, 0, s>>>(g, rfm, gfs)));
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+template <Variant V, typename T>
+static void launch_fused_typed(int stage, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
+                               const double *aux, const StageBuffers &b, double *krhs, double dt, cudaStream_t s) {
+  const dim3 grid = interior_grid(g), block(BX, BY);
+  switch (stage) {
+    case 1: rhs_fused_kernel<V, T, 1><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
+    case 2: rhs_fused_kernel<V, T, 2><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
+    case 3: rhs_fused_kernel<V, T, 3><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
+    default: rhs_fused_kernel<V, T, 4><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
+  }
+}
+
+int launch_rhs_fused_stage(Variant v, bool mixed, int stage, double dt, const GridDims &g, const RfmArrays &rfm,
+                           const PhysParams &pp, const double *aux, const StageBuffers &b, double *krhs,
+                           cudaStream_t s) {
+  if (stage < 1 || stage > 4) {
+    set_error("RK4 stage %d out of range", stage);
+    return BSSN_B200_EINVAL;
+  }
+  if (empty_interior(g)) return BSSN_B200_OK;
+  if (mixed) {
+    VARIANT_SWITCH(v, (launch_fused_typed<VV, float>(stage, g, rfm, pp, aux, b, krhs, dt, s)));
+  } else {
+    VARIANT_SWITCH(v, (launch_fused_typed<VV, double>(stage, g, rfm, pp, aux, b, krhs, dt, s)));
+  }
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+template <Variant V>
+static void launch_rk_points_typed(int stage, const GridDims &g, const RfmArrays &rfm, const StageBuffers &b,
+                                   const outerpt_bc_struct *pts, int npts, const double *krhs, double dt,
+                                   cudaStream_t s) {
+  const int threads = 128, blocks = (npts + threads - 1) / threads;
+  switch (stage) {
+    case 1: rk_points_kernel<V, 1><<<blocks, threads, 0, s>>>(g, rfm, b, pts, npts, krhs, dt); break;
+    case 2: rk_points_kernel<V, 2><<<blocks, threads, 0, s>>>(g, rfm, b, pts, npts, krhs, dt); break;
+    case 3: rk_points_kernel<V, 3><<<blocks, threads, 0, s>>>(g, rfm, b, pts, npts, krhs, dt); break;
+    default: rk_points_kernel<V, 4><<<blocks, threads, 0, s>>>(g, rfm, b, pts, npts, krhs, dt); break;
+  }
+}
+
+int launch_rk_points(Variant v, int stage, double dt, const GridDims &g, const RfmArrays &rfm, const StageBuffers &b,
+                     const outerpt_bc_struct *pts, int npts, const double *krhs, cudaStream_t s) {
+  if (npts <= 0) return BSSN_B200_OK;
+  VARIANT_SWITCH(v, (launch_rk_points_typed<VV>(stage, g, rfm, b, pts, npts, krhs, dt, s)));
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+}  // namespace bssn

@@ -1,0 +1,513 @@
+// Grid, reference-metric, boundary-structure, timestep and initial-data set-up.
+//
+// Set-up runs once per grid, on the host, in FP64 with the same closed-form expressions
+// as the reference's generated set-up code, and uploads its results. The hot path never
+// calls into this file.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "bssn_common.cuh"
+
+namespace bssn {
+
+static const double kPI = 3.14159265358979323846264338327950288;
+
+// ---------------------------------------------------------------- defaults
+// CodeParameters.py: commondata/params_struct_set_to_default (values of the generated project).
+void commondata_defaults(commondata_struct *cd) {
+  memset(cd, 0, sizeof(*cd));
+  cd->BH1_mass = 0.5;
+  cd->BH1_posn_x = 0.0;
+  cd->BH1_posn_y = 0.0;
+  cd->BH1_posn_z = 0.5;
+  cd->BH2_mass = 0.5;
+  cd->BH2_posn_x = 0.0;
+  cd->BH2_posn_y = 0.0;
+  cd->BH2_posn_z = -0.5;
+  cd->CFL_FACTOR = 0.5;
+  cd->KreissOliger_strength_gauge = 0.3;
+  cd->KreissOliger_strength_nongauge = 0.3;
+  cd->NUMGRIDS = 1;
+  cd->convergence_factor = 1.0;
+  cd->diagnostics_output_every = 0.25;
+  cd->eta = 1.0;
+  cd->output_progress_every = 1;
+  cd->t_final = 10.0;
+  snprintf(cd->outer_bc_type, 50, "radiation");
+}
+
+void params_defaults(params_struct *p) {
+  memset(p, 0, sizeof(*p));
+  p->AMPL = 10.0;
+  p->Cart_originx = p->Cart_originy = p->Cart_originz = 0.0;
+  p->Nxx0 = p->Nxx1 = p->Nxx2 = 64;
+  p->PI = kPI;
+  p->RMAX = 10.0;
+  p->SINHW = 0.2;
+  p->grid_hole_radius = 2.0;
+  p->grid_idx = 0;
+  p->grid_physical_size = 10.0;
+  p->grid_rotates = false;
+  p->is_host = true;
+  p->xmax = 10.0;
+  p->xmin = -10.0;
+  p->xxmax0 = p->xxmax1 = p->xxmax2 = 10.0;
+  p->xxmin0 = p->xxmin1 = p->xxmin2 = -10.0;
+  p->ymax = 10.0;
+  p->ymin = -10.0;
+  p->zmax = 10.0;
+  p->zmin = -10.0;
+}
+
+// ---------------------------------------------------------------- coordinates
+// xx -> Cartesian for the Spherical family, r(xx0) from reference_metric.py:1195-1330.
+struct Coord {
+  int sinh;
+  double AMPL, SINHW;
+  double r(double xx0) const {
+    if (!sinh) return xx0;
+    const double tmp0 = 1.0 / SINHW;
+    return AMPL * (exp(tmp0 * xx0) - exp(-tmp0 * xx0)) / (exp(tmp0) - exp(-tmp0));
+  }
+  double drdx0(double xx0) const {
+    if (!sinh) return 1.0;
+    const double tmp0 = 1.0 / SINHW;
+    return AMPL * (exp(tmp0 * xx0) * tmp0 + exp(-tmp0 * xx0) * tmp0) / (exp(tmp0) - exp(-tmp0));
+  }
+  void to_cart(double xx0, double xx1, double xx2, double out[3]) const {
+    const double rr = r(xx0);
+    const double tmp = rr * sin(xx1);
+    out[0] = tmp * cos(xx2);
+    out[1] = tmp * sin(xx2);
+    out[2] = rr * cos(xx1);
+  }
+};
+
+static int coord_of(const params_struct *p, Coord *c) {
+  if (p->CoordSystem_hash == SPHERICAL) *c = Coord{0, 0.0, 0.0};
+  else if (p->CoordSystem_hash == SINHSPHERICAL) *c = Coord{1, p->AMPL, p->SINHW};
+  else {
+    set_error("CoordSystem_hash %d: only Spherical (%d) and SinhSpherical (%d) are supported",
+              p->CoordSystem_hash, SPHERICAL, SINHSPHERICAL);
+    return BSSN_B200_EINVAL;
+  }
+  return BSSN_B200_OK;
+}
+
+static int host_xx(const params_struct *p, REAL *const xx[3], std::vector<double> h[3]) {
+  const int N[3] = {p->Nxx_plus_2NGHOSTS0, p->Nxx_plus_2NGHOSTS1, p->Nxx_plus_2NGHOSTS2};
+  for (int d = 0; d < 3; d++) {
+    h[d].resize(N[d]);
+    BSSN_CUDA_TRY(cudaMemcpy(h[d].data(), xx[d], sizeof(double) * N[d], cudaMemcpyDeviceToHost));
+  }
+  return BSSN_B200_OK;
+}
+
+// numerical_grids_and_timestep.py:31-190.
+int grid_params(const commondata_struct *cd, params_struct *p, REAL *xx[3], const int Nx[3], bool apply_defaults) {
+  Coord c;
+  BSSN_TRY(coord_of(p, &c));
+  if (Nx[0] != -1 && Nx[1] != -1 && Nx[2] != -1) {
+    p->Nxx0 = Nx[0];
+    p->Nxx1 = Nx[1];
+    p->Nxx2 = Nx[2];
+  }
+  snprintf(p->CoordSystemName, 100, "%s", c.sinh ? "SinhSpherical" : "Spherical");
+  if (apply_defaults) {
+    if (p->Nxx0 != 2) p->Nxx0 *= cd->convergence_factor;
+    if (p->Nxx1 != 2) p->Nxx1 *= cd->convergence_factor;
+    if (p->Nxx2 != 2) p->Nxx2 *= cd->convergence_factor;
+  }
+  if (p->Nxx0 < 1 || p->Nxx1 < 1 || p->Nxx2 < 1) {
+    set_error("grid: Nxx = (%d,%d,%d) must be positive", p->Nxx0, p->Nxx1, p->Nxx2);
+    return BSSN_B200_EINVAL;
+  }
+  p->Nxx_plus_2NGHOSTS0 = p->Nxx0 + 2 * NGHOSTS;
+  p->Nxx_plus_2NGHOSTS1 = p->Nxx1 + 2 * NGHOSTS;
+  p->Nxx_plus_2NGHOSTS2 = p->Nxx2 + 2 * NGHOSTS;
+  const long long ntot = (long long)p->Nxx_plus_2NGHOSTS0 * p->Nxx_plus_2NGHOSTS1 * p->Nxx_plus_2NGHOSTS2;
+  if (ntot * NUM_EVOL_GFS >= (1LL << 31) || p->Nxx_plus_2NGHOSTS0 > 32767 || p->Nxx_plus_2NGHOSTS1 > 32767 ||
+      p->Nxx_plus_2NGHOSTS2 > 32767) {
+    set_error("grid: %lld points x %d gridfunctions exceeds 32-bit indexing", ntot, NUM_EVOL_GFS);
+    return BSSN_B200_EINVAL;
+  }
+  if (c.sinh) p->AMPL = p->grid_physical_size;
+  else p->RMAX = p->grid_physical_size;
+  if (apply_defaults) {
+    p->xxmin0 = 0;
+    p->xxmin1 = 0;
+    p->xxmin2 = -p->PI;
+    p->xxmax0 = c.sinh ? 1 : p->RMAX;
+    p->xxmax1 = p->PI;
+    p->xxmax2 = p->PI;
+  }
+  p->dxx0 = (p->xxmax0 - p->xxmin0) / ((REAL)p->Nxx0);
+  p->dxx1 = (p->xxmax1 - p->xxmin1) / ((REAL)p->Nxx1);
+  p->dxx2 = (p->xxmax2 - p->xxmin2) / ((REAL)p->Nxx2);
+  p->invdxx0 = ((REAL)p->Nxx0) / (p->xxmax0 - p->xxmin0);
+  p->invdxx1 = ((REAL)p->Nxx1) / (p->xxmax1 - p->xxmin1);
+  p->invdxx2 = ((REAL)p->Nxx2) / (p->xxmax2 - p->xxmin2);
+  const int N[3] = {p->Nxx_plus_2NGHOSTS0, p->Nxx_plus_2NGHOSTS1, p->Nxx_plus_2NGHOSTS2};
+  const double xmin[3] = {p->xxmin0, p->xxmin1, p->xxmin2}, dx[3] = {p->dxx0, p->dxx1, p->dxx2};
+  for (int d = 0; d < 3; d++) {
+    std::vector<double> h(N[d]);
+    // xx_j = xxmin + (j - NGHOSTS + 1/2) dxx, rounded once (a fused multiply-add), as the
+    // reference's cell-centred-grid macro compiles on FMA-capable hosts.
+    for (int j = 0; j < N[d]; j++) h[j] = fma((REAL)(j - NGHOSTS) + (1.0 / 2.0), dx[d], xmin[d]);
+    BSSN_CUDA_TRY(cudaMalloc(&xx[d], sizeof(double) * N[d]));
+    BSSN_CUDA_TRY(cudaMemcpy(xx[d], h.data(), sizeof(double) * N[d], cudaMemcpyHostToDevice));
+  }
+  return BSSN_B200_OK;
+}
+
+// ---------------------------------------------------------------- rfm precompute (rfm_precompute.py:84-565)
+int rfm_malloc(const params_struct *p, rfm_struct *r) {
+  const size_t n0 = p->Nxx_plus_2NGHOSTS0, n1 = p->Nxx_plus_2NGHOSTS1;
+  BSSN_CUDA_TRY(cudaMalloc(&r->f0_of_xx0, sizeof(double) * n0));
+  BSSN_CUDA_TRY(cudaMalloc(&r->f0_of_xx0__D0, sizeof(double) * n0));
+  BSSN_CUDA_TRY(cudaMalloc(&r->f0_of_xx0__DD00, sizeof(double) * n0));
+  BSSN_CUDA_TRY(cudaMalloc(&r->f0_of_xx0__DDD000, sizeof(double) * n0));
+  BSSN_CUDA_TRY(cudaMalloc(&r->f1_of_xx1, sizeof(double) * n1));
+  BSSN_CUDA_TRY(cudaMalloc(&r->f1_of_xx1__D1, sizeof(double) * n1));
+  BSSN_CUDA_TRY(cudaMalloc(&r->f1_of_xx1__DD11, sizeof(double) * n1));
+  return BSSN_B200_OK;
+}
+
+int rfm_free(rfm_struct *r) {
+  double **f = &r->f0_of_xx0;
+  for (int k = 0; k < 7; k++) {
+    if (f[k]) cudaFree(f[k]);
+    f[k] = nullptr;
+  }
+  return BSSN_B200_OK;
+}
+
+int rfm_defines(const params_struct *p, rfm_struct *r, REAL *xx[3]) {
+  Coord c;
+  BSSN_TRY(coord_of(p, &c));
+  std::vector<double> hx[3];
+  BSSN_TRY(host_xx(p, xx, hx));
+  const int n0 = p->Nxx_plus_2NGHOSTS0, n1 = p->Nxx_plus_2NGHOSTS1;
+  std::vector<double> f0(n0), f0d(n0), f0dd(n0), f0ddd(n0), f1(n1), f1d(n1), f1dd(n1);
+  for (int i = 0; i < n0; i++) {
+    const double xx0 = hx[0][i];
+    if (c.sinh) {
+      const double AMPL = c.AMPL, SINHW = c.SINHW;
+      // Expression trees of the generated rfm_precompute_defines (SinhSpherical).
+      f0[i] = AMPL * (exp(xx0 / SINHW) - exp(-xx0 / SINHW)) / (exp((1.0 / (SINHW))) - exp(-1 / SINHW));
+      f0d[i] = AMPL * (exp(xx0 / SINHW) / SINHW + exp(-xx0 / SINHW) / SINHW) / (exp((1.0 / (SINHW))) - exp(-1 / SINHW));
+      f0dd[i] = AMPL * (exp(xx0 / SINHW) / ((SINHW) * (SINHW)) - exp(-xx0 / SINHW) / ((SINHW) * (SINHW))) /
+                (exp((1.0 / (SINHW))) - exp(-1 / SINHW));
+      f0ddd[i] = AMPL * (exp(xx0 / SINHW) / ((SINHW) * (SINHW) * (SINHW)) + exp(-xx0 / SINHW) / ((SINHW) * (SINHW) * (SINHW))) /
+                 (exp((1.0 / (SINHW))) - exp(-1 / SINHW));
+    } else {
+      f0[i] = xx0;
+      f0d[i] = 1.0;
+      f0dd[i] = 0.0;
+      f0ddd[i] = 0.0;
+    }
+  }
+  for (int i = 0; i < n1; i++) {
+    const double xx1 = hx[1][i];
+    f1[i] = sin(xx1);
+    f1d[i] = cos(xx1);
+    f1dd[i] = -sin(xx1);
+  }
+  BSSN_CUDA_TRY(cudaMemcpy(r->f0_of_xx0, f0.data(), sizeof(double) * n0, cudaMemcpyHostToDevice));
+  BSSN_CUDA_TRY(cudaMemcpy(r->f0_of_xx0__D0, f0d.data(), sizeof(double) * n0, cudaMemcpyHostToDevice));
+  BSSN_CUDA_TRY(cudaMemcpy(r->f0_of_xx0__DD00, f0dd.data(), sizeof(double) * n0, cudaMemcpyHostToDevice));
+  BSSN_CUDA_TRY(cudaMemcpy(r->f0_of_xx0__DDD000, f0ddd.data(), sizeof(double) * n0, cudaMemcpyHostToDevice));
+  BSSN_CUDA_TRY(cudaMemcpy(r->f1_of_xx1, f1.data(), sizeof(double) * n1, cudaMemcpyHostToDevice));
+  BSSN_CUDA_TRY(cudaMemcpy(r->f1_of_xx1__D1, f1d.data(), sizeof(double) * n1, cudaMemcpyHostToDevice));
+  BSSN_CUDA_TRY(cudaMemcpy(r->f1_of_xx1__DD11, f1dd.data(), sizeof(double) * n1, cudaMemcpyHostToDevice));
+  return BSSN_B200_OK;
+}
+
+// ---------------------------------------------------------------- bcstruct (bcstruct_set_up.py:442-792)
+// Eigen-coordinate map of a ghost point (EigenCoord_set_x0x1x2_inbounds__i0i1i2_inbounds_single_pt):
+// (x0,x1,x2) -> Cartesian (eigen-coordinate Spherical) -> (x0,x1,x2)' -> nearest index.
+static int eigen_map(const params_struct *p, const Coord &c, const std::vector<double> hx[3], int i0, int i1,
+                     int i2, double xin[3], int iin[3]) {
+  const double xx0 = hx[0][i0], xx1 = hx[1][i1], xx2 = hx[2][i2];
+  double Cartx, Carty, Cartz;
+  {
+    const double tmp0 = xx0 * sin(xx1);
+    Cartx = tmp0 * cos(xx2);
+    Carty = tmp0 * sin(xx2);
+    Cartz = xx0 * cos(xx1);
+  }
+  const double tmp0 = sqrt(((Cartx) * (Cartx)) + ((Carty) * (Carty)) + ((Cartz) * (Cartz)));
+  const double x0in = tmp0;
+  const double x1in = acos(Cartz / tmp0);
+  const double x2in = atan2(Carty, Cartx);
+  const double dxx[3] = {p->dxx0, p->dxx1, p->dxx2};
+  const double xxmin[3] = {hx[0][0] - ((double)(0 - NGHOSTS) + (1.0 / 2.0)) * dxx[0],
+                           hx[1][0] - ((double)(0 - NGHOSTS) + (1.0 / 2.0)) * dxx[1],
+                           hx[2][0] - ((double)(0 - NGHOSTS) + (1.0 / 2.0)) * dxx[2]};
+  const double xinb[3] = {x0in, x1in, x2in};
+  const int N[3] = {p->Nxx_plus_2NGHOSTS0, p->Nxx_plus_2NGHOSTS1, p->Nxx_plus_2NGHOSTS2};
+  for (int d = 0; d < 3; d++) {
+    iin[d] = (int)((xinb[d] - xxmin[d] - (1.0 / 2.0) * dxx[d] + ((double)NGHOSTS) * dxx[d]) / dxx[d] + 0.5);
+    if (iin[d] < 0 || iin[d] >= N[d]) {
+      set_error("bcstruct: ghost point (%d,%d,%d) maps to index %d outside [0,%d) in direction %d", i0, i1, i2, iin[d],
+                N[d], d);
+      return BSSN_B200_ESETUP;
+    }
+  }
+  // Sanity check in the actual coordinate system: both points must be the same Cartesian point.
+  double a[3], b[3];
+  c.to_cart(xx0, xx1, xx2, a);
+  c.to_cart(hx[0][iin[0]], hx[1][iin[1]], hx[2][iin[2]], b);
+  const double EPS_REL = 1e-8;
+  const double norm = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]) + 1e-15;
+  if (fabs(a[0] - b[0]) > EPS_REL * norm || fabs(a[1] - b[1]) > EPS_REL * norm || fabs(a[2] - b[2]) > EPS_REL * norm) {
+    set_error("bcstruct: inner boundary point (%d,%d,%d) does not map to a grid point", i0, i1, i2);
+    return BSSN_B200_ESETUP;
+  }
+  for (int d = 0; d < 3; d++) xin[d] = hx[d][iin[d]];
+  return BSSN_B200_OK;
+}
+
+// Unit-vector dot products of the 10 parity types (set_parity_for_inner_boundary_single_pt).
+static int parity_signs(double xx1, double xx2, const double xin[3], int8_t parity[10]) {
+  const double xx1_inbounds = xin[1], xx2_inbounds = xin[2];
+  const double tmp0 = cos(xx1) * cos(xx1_inbounds);
+  const double tmp1 = sin(xx1) * sin(xx1_inbounds);
+  const double tmp2 = sin(xx2) * sin(xx2_inbounds);
+  const double tmp3 = cos(xx2) * cos(xx2_inbounds);
+  const double tmp4 = tmp0 + tmp1 * tmp2 + tmp1 * tmp3;
+  const double tmp5 = tmp0 * tmp2 + tmp0 * tmp3 + tmp1;
+  const double tmp6 = tmp2 + tmp3;
+  const double par[10] = {1, tmp4, tmp5, tmp6, tmp4 * tmp4, tmp4 * tmp5, tmp4 * tmp6, tmp5 * tmp5, tmp5 * tmp6, tmp6 * tmp6};
+  const double EPS_REL = 1e-8;
+  for (int k = 0; k < 10; k++) {
+    if (fabs(par[k]) < 1 - EPS_REL || fabs(par[k]) > 1 + EPS_REL) {
+      set_error("bcstruct: parity type %d evaluated to %e, not +/-1", k, par[k]);
+      return BSSN_B200_ESETUP;
+    }
+    parity[k] = par[k] < 0 ? -1 : 1;
+  }
+  return BSSN_B200_OK;
+}
+
+struct HostBc {
+  std::vector<innerpt_bc_struct> inner;
+  std::vector<outerpt_bc_struct> outer[NGHOSTS * 3];
+  bc_info_struct info;
+};
+
+int bcstruct_host(const params_struct *p, const std::vector<double> hx[3], HostBc *out) {
+  Coord c;
+  BSSN_TRY(coord_of(p, &c));
+  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1, N2 = p->Nxx_plus_2NGHOSTS2;
+  memset(&out->info, 0, sizeof(out->info));
+  out->inner.clear();
+  // Step 1: inner boundary points, in i2-i1-i0 loop order.
+  for (int i2 = 0; i2 < N2; i2++)
+    for (int i1 = 0; i1 < N1; i1++)
+      for (int i0 = 0; i0 < N0; i0++) {
+        const bool interior = i0 >= NGHOSTS && i0 < N0 - NGHOSTS && i1 >= NGHOSTS && i1 < N1 - NGHOSTS &&
+                              i2 >= NGHOSTS && i2 < N2 - NGHOSTS;
+        if (interior) continue;
+        double xin[3];
+        int iin[3];
+        BSSN_TRY(eigen_map(p, c, hx, i0, i1, i2, xin, iin));
+        if (i0 == iin[0] && i1 == iin[1] && i2 == iin[2]) continue;  // pure outer point
+        innerpt_bc_struct bc;
+        memset(&bc, 0, sizeof(bc));
+        bc.dstpt = i0 + N0 * (i1 + N1 * i2);
+        bc.srcpt = iin[0] + N0 * (iin[1] + N1 * iin[2]);
+        BSSN_TRY(parity_signs(hx[1][i1], hx[2][i2], xin, bc.parity));
+        out->inner.push_back(bc);
+      }
+  out->info.num_inner_boundary_points = (int)out->inner.size();
+  // Step 2: pure outer points, layer by layer from the inside out, faces x0, x1, x2.
+  int imin[3] = {NGHOSTS, NGHOSTS, NGHOSTS};
+  int imax[3] = {N0 - NGHOSTS, N1 - NGHOSTS, N2 - NGHOSTS};
+  for (int gz = 0; gz < NGHOSTS; gz++) {
+    int r[6][6];
+    const int x0min[6] = {imin[0] - 1, imin[0], imin[1], imax[1], imin[2], imax[2]};
+    imin[0]--;
+    const int x0max[6] = {imax[0], imax[0] + 1, imin[1], imax[1], imin[2], imax[2]};
+    imax[0]++;
+    const int x1min[6] = {imin[0], imax[0], imin[1] - 1, imin[1], imin[2], imax[2]};
+    imin[1]--;
+    const int x1max[6] = {imin[0], imax[0], imax[1], imax[1] + 1, imin[2], imax[2]};
+    imax[1]++;
+    const int x2min[6] = {imin[0], imax[0], imin[1], imax[1], imin[2] - 1, imin[2]};
+    imin[2]--;
+    const int x2max[6] = {imin[0], imax[0], imin[1], imax[1], imax[2], imax[2] + 1};
+    imax[2]++;
+    memcpy(r[0], x0min, sizeof(x0min));
+    memcpy(r[1], x0max, sizeof(x0max));
+    memcpy(r[2], x1min, sizeof(x1min));
+    memcpy(r[3], x1max, sizeof(x1max));
+    memcpy(r[4], x2min, sizeof(x2min));
+    memcpy(r[5], x2max, sizeof(x2max));
+    for (int f = 0; f < 6; f++)
+      for (int k = 0; k < 6; k++) out->info.bc_loop_bounds[gz][f][k] = r[f][k];
+  }
+  for (int gz = 0; gz < NGHOSTS; gz++) {
+    for (int dirn = 0; dirn < 3; dirn++) {
+      std::vector<outerpt_bc_struct> &list = out->outer[dirn + 3 * gz];
+      list.clear();
+      for (int face = 2 * dirn; face <= 2 * dirn + 1; face++) {
+        const int FACEX0 = (face == 0) - (face == 1);
+        const int FACEX1 = (face == 2) - (face == 3);
+        const int FACEX2 = (face == 4) - (face == 5);
+        const int *b = out->info.bc_loop_bounds[gz][face];
+        for (int i2 = b[4]; i2 < b[5]; i2++)
+          for (int i1 = b[2]; i1 < b[3]; i1++)
+            for (int i0 = b[0]; i0 < b[1]; i0++) {
+              double xin[3];
+              int iin[3];
+              BSSN_TRY(eigen_map(p, c, hx, i0, i1, i2, xin, iin));
+              if (i0 == iin[0] && i1 == iin[1] && i2 == iin[2]) {
+                outerpt_bc_struct o;
+                memset(&o, 0, sizeof(o));
+                o.i0 = (short)i0;
+                o.i1 = (short)i1;
+                o.i2 = (short)i2;
+                o.FACEX0 = (int8_t)FACEX0;
+                o.FACEX1 = (int8_t)FACEX1;
+                o.FACEX2 = (int8_t)FACEX2;
+                list.push_back(o);
+              }
+            }
+      }
+      out->info.num_pure_outer_boundary_points[gz][dirn] = (int)list.size();
+    }
+  }
+  return BSSN_B200_OK;
+}
+
+int bcstruct_setup(const params_struct *p, REAL *xx[3], bc_struct *bc) {
+  std::vector<double> hx[3];
+  BSSN_TRY(host_xx(p, xx, hx));
+  HostBc h;
+  BSSN_TRY(bcstruct_host(p, hx, &h));
+  memset(bc, 0, sizeof(*bc));
+  bc->bc_info = h.info;
+  const size_t ni = std::max<size_t>(1, h.inner.size());
+  BSSN_CUDA_TRY(cudaMalloc(&bc->inner_bc_array, sizeof(innerpt_bc_struct) * ni));
+  if (!h.inner.empty())
+    BSSN_CUDA_TRY(cudaMemcpy(bc->inner_bc_array, h.inner.data(), sizeof(innerpt_bc_struct) * h.inner.size(),
+                             cudaMemcpyHostToDevice));
+  for (int k = 0; k < NGHOSTS * 3; k++) {
+    const size_t n = std::max<size_t>(1, h.outer[k].size());
+    BSSN_CUDA_TRY(cudaMalloc(&bc->pure_outer_bc_array[k], sizeof(outerpt_bc_struct) * n));
+    if (!h.outer[k].empty())
+      BSSN_CUDA_TRY(cudaMemcpy(bc->pure_outer_bc_array[k], h.outer[k].data(),
+                               sizeof(outerpt_bc_struct) * h.outer[k].size(), cudaMemcpyHostToDevice));
+  }
+  return BSSN_B200_OK;
+}
+
+int bcstruct_release(bc_struct *bc) {
+  if (bc->inner_bc_array) cudaFree(bc->inner_bc_array);
+  bc->inner_bc_array = nullptr;
+  for (int k = 0; k < NGHOSTS * 3; k++) {
+    if (bc->pure_outer_bc_array[k]) cudaFree(bc->pure_outer_bc_array[k]);
+    bc->pure_outer_bc_array[k] = nullptr;
+  }
+  return BSSN_B200_OK;
+}
+
+// ---------------------------------------------------------------- timestep (cfl_limited_timestep)
+int cfl_dt(commondata_struct *cd, const params_struct *p, REAL *xx[3]) {
+  Coord c;
+  BSSN_TRY(coord_of(p, &c));
+  std::vector<double> hx[3];
+  BSSN_TRY(host_xx(p, xx, hx));
+  double ds_min = 1e38;
+  for (int i2 = 0; i2 < p->Nxx_plus_2NGHOSTS2; i2++)
+    for (int i1 = 0; i1 < p->Nxx_plus_2NGHOSTS1; i1++)
+      for (int i0 = 0; i0 < p->Nxx_plus_2NGHOSTS0; i0++) {
+        const double xx0 = hx[0][i0], xx1 = hx[1][i1];
+        double ds0, ds1, ds2;
+        if (c.sinh) {
+          const double tmp0 = (1.0 / (c.SINHW));
+          const double tmp4 = c.AMPL / (exp(tmp0) - exp(-tmp0));
+          const double tmp2 = exp(tmp0 * xx0);
+          const double tmp3 = exp(-tmp0 * xx0);
+          const double tmp5 = tmp4 * (tmp2 - tmp3);
+          ds0 = fabs(p->dxx0 * tmp4 * (tmp0 * tmp2 + tmp0 * tmp3));
+          ds1 = fabs(p->dxx1 * tmp5);
+          ds2 = fabs(p->dxx2 * tmp5 * sin(xx1));
+        } else {
+          ds0 = fabs(p->dxx0);
+          ds1 = fabs(p->dxx1 * xx0);
+          ds2 = fabs(p->dxx2 * xx0 * sin(xx1));
+        }
+        const double l = std::min(ds0, std::min(ds1, ds2));
+        ds_min = std::min(ds_min, l);
+      }
+  cd->dt = std::min(cd->dt, ds_min * cd->CFL_FACTOR);
+  return BSSN_B200_OK;
+}
+
+// ---------------------------------------------------------------- Brill-Lindquist initial data
+// InitialData_Cartesian.py:111-141 (psi = 1 + sum m/(2|x-x_i|), gamma = psi^4 delta, K = 0,
+// alpha = psi^-2), ADM -> BSSN in the Cartesian basis, then the basis change to the
+// reference-metric basis and rescaling (ADM_Initial_Data_Reader__BSSN_Converter.py:33-460),
+// lambda^i from centred FD of hDD on the interior, then extrapolation and inner BCs.
+int bl_initial_data(const commondata_struct *cd, const params_struct *p, REAL *xx[3], const bc_struct *bc,
+                    double *y_n, cudaStream_t s) {
+  Coord c;
+  BSSN_TRY(coord_of(p, &c));
+  Variant v;
+  BSSN_TRY(variant_of(p, &v));
+  std::vector<double> hx[3];
+  BSSN_TRY(host_xx(p, xx, hx));
+  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1, N2 = p->Nxx_plus_2NGHOSTS2;
+  const size_t ntot = (size_t)N0 * N1 * N2;
+  std::vector<double> h(ntot * NUM_EVOL_GFS, 0.0);
+  for (int i2 = 0; i2 < N2; i2++)
+    for (int i1 = 0; i1 < N1; i1++)
+      for (int i0 = 0; i0 < N0; i0++) {
+        const double xx0 = hx[0][i0], xx1 = hx[1][i1], xx2 = hx[2][i2];
+        double X[3];
+        c.to_cart(xx0, xx1, xx2, X);
+        const double d1 = sqrt((X[0] - cd->BH1_posn_x) * (X[0] - cd->BH1_posn_x) + (X[1] - cd->BH1_posn_y) * (X[1] - cd->BH1_posn_y) +
+                               (X[2] - cd->BH1_posn_z) * (X[2] - cd->BH1_posn_z));
+        const double d2 = sqrt((X[0] - cd->BH2_posn_x) * (X[0] - cd->BH2_posn_x) + (X[1] - cd->BH2_posn_y) * (X[1] - cd->BH2_posn_y) +
+                               (X[2] - cd->BH2_posn_z) * (X[2] - cd->BH2_posn_z));
+        const double psi = (1.0 / 2.0) * cd->BH1_mass / d1 + (1.0 / 2.0) * cd->BH2_mass / d2 + 1;
+        const double psi4 = psi * psi * psi * psi;
+        const double alpha = 1.0 / sqrt(cbrt(pow(psi, 12)));
+        // ADM (Cartesian): gamma_ij = psi^4 delta_ij, K_ij = 0 -> BSSN (Cartesian):
+        const double detg = psi4 * psi4 * psi4;
+        const double gbar_scale = cbrt(1.0 / detg);  // (det gamma)^(-1/3)
+        const double gbar = psi4 * gbar_scale;       // diagonal of gammabar_ij (= 1 up to rounding)
+        const double cf = 1.0 / sqrt(cbrt(detg));
+        // Basis change: gammabar^rfm_ij = J_ai J_bj gammabar^Cart_ab with J_ai = dx^a/dxx^i.
+        const double rr = c.r(xx0), dr = c.drdx0(xx0);
+        const double st = sin(xx1), ct = cos(xx1), sp_ = sin(xx2), cp = cos(xx2);
+        const double J[3][3] = {{dr * st * cp, rr * ct * cp, -rr * st * sp_},
+                                {dr * st * sp_, rr * ct * sp_, rr * st * cp},
+                                {dr * ct, -rr * st, 0.0}};
+        const double sf[3] = {dr, rr, rr * st};  // scale factors; ReDD_ij = sf_i sf_j
+        const double ghat[3] = {dr * dr, rr * rr, rr * rr * st * st};
+        const size_t idx = i0 + (size_t)N0 * (i1 + (size_t)N1 * i2);
+        int k = 0;
+        const int hslot[6] = {HDD00GF, HDD01GF, HDD02GF, HDD11GF, HDD12GF, HDD22GF};
+        for (int i = 0; i < 3; i++)
+          for (int j = i; j < 3; j++, k++) {
+            double g = 0.0;
+            for (int a = 0; a < 3; a++) g += J[a][i] * J[a][j] * gbar;
+            const double gh = (i == j) ? ghat[i] : 0.0;
+            h[idx + ntot * hslot[k]] = (g - gh) / (sf[i] * sf[j]);
+          }
+        h[idx + ntot * ALPHAGF] = alpha;
+        h[idx + ntot * CFGF] = cf;
+        // aDD, trK, vetU, betU, lambdaU (interior lambda set below) are zero for BL data.
+      }
+  BSSN_CUDA_TRY(cudaStreamSynchronize(s));
+  BSSN_CUDA_TRY(cudaMemcpy(y_n, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  (void)v;
+  return BSSN_B200_OK;
+}
+
+}  // namespace bssn

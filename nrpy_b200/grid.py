@@ -1,0 +1,262 @@
+"""Host-side driver of one BHaH BSSN grid on a B200, through the C ABI.
+
+Mirrors the set-up sequence of the reference's generated main()
+(nrpy/infrastructures/BHaH/main_c.py:125-343): CodeParameter defaults ->
+numerical_grid_params_Nxx_dxx_xx -> rfm_precompute -> bcstruct_set_up ->
+cfl_limited_timestep -> gridfunction storage -> initial_data, then
+MoL_step_forward_in_time per step. Gridfunction storage is owned by torch tensors on the
+GPU (device memory and streams only; all arithmetic runs in libbssn_b200).
+"""
+
+import ctypes as C
+from typing import Dict, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import lib as L
+
+
+def _ptr(t: torch.Tensor):
+    assert t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()
+    return C.cast(C.c_void_p(t.data_ptr()), L.PR)
+
+
+class BSSNGrid:
+    """One single-patch Spherical or SinhSpherical grid with RK4 storage on the GPU.
+
+    Arguments follow the reference's CodeParameters: ``Nxx`` interior points per
+    direction, ``grid_physical_size`` (RMAX for Spherical, AMPL for SinhSpherical),
+    ``SINHW``, Brill-Lindquist masses / z positions, ``CFL_FACTOR``, ``outer_bc_type``
+    ("radiation" or "extrapolation") and ``symmetry_axes`` ("" or "2").
+    """
+
+    def __init__(
+        self,
+        coord: str = "Spherical",
+        Nxx: Sequence[int] = (72, 12, 2),
+        grid_physical_size: float = 7.5,
+        SINHW: float = 0.2,
+        BH1_mass: float = 0.5,
+        BH1_posn_z: float = 0.5,
+        BH2_mass: float = 0.5,
+        BH2_posn_z: float = -0.5,
+        CFL_FACTOR: float = 0.5,
+        eta: float = 1.0,
+        outer_bc_type: str = "radiation",
+        symmetry_axes: str = "",
+        initial_data: bool = True,
+        device: Optional[torch.device] = None,
+    ):
+        if coord not in L.COORD_HASH:
+            raise ValueError(f"CoordSystem {coord!r} not supported; choose from {sorted(L.COORD_HASH)}")
+        self.lib = L.load()
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        torch.cuda.set_device(self.device)
+        L.check(self.lib.bssn_b200_set_symmetry_axes(symmetry_axes.encode()))
+        self.symmetry_axes = symmetry_axes
+        self.coord = coord
+        self.cd = L.CommondataStruct()
+        self.gd = (L.GriddataStruct * L.MAXNUMGRIDS)()
+        self.lib.commondata_struct_set_to_default(C.byref(self.cd))
+        self.lib.params_struct_set_to_default(C.byref(self.cd), self.gd)
+        cd = self.cd
+        cd.BH1_mass, cd.BH1_posn_z, cd.BH2_mass, cd.BH2_posn_z = BH1_mass, BH1_posn_z, BH2_mass, BH2_posn_z
+        cd.CFL_FACTOR = CFL_FACTOR
+        cd.eta = eta
+        cd.outer_bc_type = outer_bc_type.encode()
+        cd.NUMGRIDS = 1
+        g = self.gd[0]
+        p = g.params
+        p.CoordSystem_hash = L.COORD_HASH[coord]
+        p.grid_physical_size = grid_physical_size
+        p.SINHW = SINHW
+        p.grid_idx = 0
+        p.gridname = f"grid_{coord}".encode()
+        Nx = (C.c_int * 3)(*Nxx)
+        self.lib.numerical_grid_params_Nxx_dxx_xx(C.byref(cd), C.byref(g.params), g.xx, Nx, True)
+        self._rfm = L.RfmStruct()
+        g.rfmstruct = C.pointer(self._rfm)
+        self.lib.rfm_precompute_malloc(C.byref(cd), C.byref(g.params), g.rfmstruct)
+        self.lib.rfm_precompute_defines(C.byref(cd), C.byref(g.params), g.rfmstruct, g.xx)
+        self.lib.bcstruct_set_up(C.byref(cd), C.byref(g.params), g.xx, C.byref(g.bcstruct))
+        cd.dt = 1e30
+        self.lib.cfl_limited_timestep(C.byref(cd), C.byref(g.params), g.xx)
+        cd.nn = cd.nn_0 = 0
+        cd.t_0 = cd.time = 0.0
+        self.N = (p.Nxx_plus_2NGHOSTS0, p.Nxx_plus_2NGHOSTS1, p.Nxx_plus_2NGHOSTS2)
+        self.ntot = self.N[0] * self.N[1] * self.N[2]
+        self.n_interior = p.Nxx0 * p.Nxx1 * p.Nxx2
+        ev = L.NUM_EVOL_GFS * self.ntot
+        mk = lambda n: torch.zeros(n, dtype=torch.float64, device=self.device)  # noqa: E731
+        self.y_n = mk(ev)
+        self.run = mk(ev)
+        self.k_odd = mk(ev)
+        self.k_even = mk(ev)
+        self.aux = mk(L.NUM_AUXEVOL_GFS * self.ntot)
+        self.diag = mk(L.NUM_DIAG_GFS * self.ntot)
+        gf = g.gridfuncs
+        gf.y_n_gfs, gf.y_nplus1_running_total_gfs = _ptr(self.y_n), _ptr(self.run)
+        gf.k_odd_gfs, gf.k_even_gfs, gf.auxevol_gfs = _ptr(self.k_odd), _ptr(self.k_even), _ptr(self.aux)
+        self._stepper = None
+        if initial_data:
+            self.lib.initial_data(C.byref(cd), self.gd)
+
+    # ------------------------------------------------------------------ accessors
+    @property
+    def params(self) -> L.ParamsStruct:
+        return self.gd[0].params
+
+    @property
+    def dt(self) -> float:
+        return self.cd.dt
+
+    @property
+    def stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def view(self, t: torch.Tensor, ngfs: Optional[int] = None) -> torch.Tensor:
+        n = t.numel() // self.ntot if ngfs is None else ngfs
+        return t.view(n, self.N[2], self.N[1], self.N[0])
+
+    def interior(self, t: torch.Tensor) -> torch.Tensor:
+        G = L.NGHOSTS
+        return self.view(t)[:, G:-G, G:-G, G:-G]
+
+    def device_array(self, ptr, n: int, ctype=C.c_double) -> np.ndarray:
+        """Copy n elements of a library-owned device array to a host numpy array."""
+        out = np.zeros(n, dtype=np.dtype(ctype))
+        if n:
+            L.check(self.lib.bssn_b200_memcpy(out.ctypes.data_as(C.c_void_p), C.cast(ptr, C.c_void_p),
+                                              out.nbytes, 1))
+        return out
+
+    def xx(self) -> Sequence[np.ndarray]:
+        return [self.device_array(self.gd[0].xx[d], self.N[d]) for d in range(3)]
+
+    def rfm(self) -> Dict[str, np.ndarray]:
+        out = {}
+        for name, _ in L.RfmStruct._fields_:
+            n = self.N[0] if name.startswith("f0") else self.N[1]
+            out[name] = self.device_array(getattr(self._rfm, name), n)
+        return out
+
+    def bcstruct(self):
+        """Host copies of (inner_bc_array, {(gz, dirn): outer list}, bc_info)."""
+        bc = self.gd[0].bcstruct
+        ni = bc.bc_info.num_inner_boundary_points
+        inner = (L.InnerptBcStruct * max(ni, 1))()
+        if ni:
+            L.check(self.lib.bssn_b200_memcpy(C.cast(inner, C.c_void_p), C.cast(bc.inner_bc_array, C.c_void_p),
+                                              C.sizeof(L.InnerptBcStruct) * ni, 1))
+        outer = {}
+        for gz in range(L.NGHOSTS):
+            for d in range(3):
+                n = bc.bc_info.num_pure_outer_boundary_points[gz][d]
+                arr = (L.OuterptBcStruct * max(n, 1))()
+                if n:
+                    L.check(self.lib.bssn_b200_memcpy(C.cast(arr, C.c_void_p),
+                                                      C.cast(bc.pure_outer_bc_array[d + 3 * gz], C.c_void_p),
+                                                      C.sizeof(L.OuterptBcStruct) * n, 1))
+                outer[(gz, d)] = arr[:n]
+        return inner[:ni], outer, bc.bc_info
+
+    # ------------------------------------------------------------------ operators
+    def ricci_eval(self, in_gfs: torch.Tensor, aux: torch.Tensor) -> None:
+        g = self.gd[0]
+        L.check(self.lib.bssn_b200_ricci_eval(C.byref(g.params), g.rfmstruct, _ptr(in_gfs), _ptr(aux), self.stream))
+
+    def rhs_eval(self, aux: torch.Tensor, in_gfs: torch.Tensor, rhs: torch.Tensor, mixed: bool = False) -> None:
+        g = self.gd[0]
+        f = self.lib.bssn_b200_rhs_eval_mixed if mixed else self.lib.bssn_b200_rhs_eval
+        L.check(f(C.byref(self.cd), C.byref(g.params), g.rfmstruct, _ptr(aux), _ptr(in_gfs), _ptr(rhs), self.stream))
+
+    def apply_bcs_outerradiation_and_inner(self, gfs: torch.Tensor, rhs: torch.Tensor) -> None:
+        g = self.gd[0]
+        L.check(self.lib.bssn_b200_apply_bcs_outerradiation_and_inner(
+            C.byref(self.cd), C.byref(g.params), C.byref(g.bcstruct), g.xx, None, None, _ptr(gfs), _ptr(rhs),
+            self.stream))
+
+    def apply_bcs_outerextrap_and_inner(self, gfs: torch.Tensor) -> None:
+        g = self.gd[0]
+        L.check(self.lib.bssn_b200_apply_bcs_outerextrap_and_inner(C.byref(g.params), C.byref(g.bcstruct),
+                                                                   _ptr(gfs), self.stream))
+
+    def apply_bcs_inner_only(self, gfs: torch.Tensor, parity_types: Optional[Sequence[int]] = None) -> None:
+        g = self.gd[0]
+        n = gfs.numel() // self.ntot
+        par = None
+        if parity_types is not None:
+            par = (C.c_int8 * len(parity_types))(*parity_types)
+        L.check(self.lib.bssn_b200_apply_bcs_inner_only(C.byref(g.params), C.byref(g.bcstruct), _ptr(gfs), n,
+                                                        par, self.stream))
+
+    def enforce_detgammabar_equals_detgammahat(self, gfs: torch.Tensor) -> None:
+        g = self.gd[0]
+        L.check(self.lib.bssn_b200_enforce_detgammabar_equals_detgammahat(C.byref(g.params), g.rfmstruct,
+                                                                          _ptr(gfs), self.stream))
+
+    def constraints_eval(self, in_gfs: Optional[torch.Tensor] = None, diag: Optional[torch.Tensor] = None):
+        """H, M^2, |Lambda| on the interior (Ricci recomputed from in_gfs into the aux buffer)."""
+        in_gfs = self.y_n if in_gfs is None else in_gfs
+        diag = self.diag if diag is None else diag
+        g = self.gd[0]
+        self.ricci_eval(in_gfs, self.aux)
+        L.check(self.lib.bssn_b200_constraints_eval(C.byref(self.cd), C.byref(g.params), g.rfmstruct, _ptr(in_gfs),
+                                                    _ptr(self.aux), _ptr(diag), self.stream))
+        return diag
+
+    def constraint_norms(self, in_gfs: Optional[torch.Tensor] = None) -> Dict[str, float]:
+        """Volume-weighted L2 norms sqrt(sum f^2 dV) and RMS of H, M^2, |Lambda| over the interior."""
+        diag = self.constraints_eval(in_gfs)
+        out = (C.c_double * 4)()
+        g = self.gd[0]
+        L.check(self.lib.bssn_b200_constraint_integrals(C.byref(g.params), g.rfmstruct, _ptr(diag), out,
+                                                        self.stream))
+        vol = out[3]
+        names = ["H", "MSQUARED", "LAMBDA_CONSTRAINT"]
+        res = {f"{n}_L2": float(np.sqrt(out[k])) for k, n in enumerate(names)}
+        res.update({f"{n}_RMS": float(np.sqrt(out[k] / vol)) if vol > 0 else 0.0 for k, n in enumerate(names)})
+        res["volume"] = vol
+        return res
+
+    # ------------------------------------------------------------------ time stepping
+    def MoL_step_forward_in_time(self, mode: int = 1, mixed: bool = False, nsteps: int = 1) -> None:
+        for _ in range(nsteps):
+            L.check(self.lib.bssn_b200_mol_step(C.byref(self.cd), self.gd, mode, int(mixed), self.stream))
+
+    def make_stepper(self, mode: int = 1, mixed: bool = False, steps_per_graph: int = 1, stream=None):
+        """Capture `steps_per_graph` RK4 steps into a CUDA graph bound to this grid's buffers."""
+        self.free_stepper()
+        st = C.c_void_p()
+        s = stream if stream is not None else torch.cuda.Stream(self.device)
+        self._stepper_stream = s
+        L.check(self.lib.bssn_b200_stepper_create(C.byref(self.cd), self.gd, mode, int(mixed), steps_per_graph,
+                                                  C.c_void_p(s.cuda_stream), C.byref(st)))
+        self._stepper = st
+        self._steps_per_graph = steps_per_graph
+        return s
+
+    def run_stepper(self, graph_launches: int) -> None:
+        if self._stepper is None:
+            raise RuntimeError("make_stepper() first")
+        L.check(self.lib.bssn_b200_stepper_run(self._stepper, graph_launches))
+
+    def free_stepper(self) -> None:
+        if getattr(self, "_stepper", None) is not None:
+            self.lib.bssn_b200_stepper_destroy(self._stepper)
+            self._stepper = None
+
+    def close(self) -> None:
+        self.free_stepper()
+        g = self.gd[0]
+        if getattr(self, "_rfm", None) is not None:
+            self.lib.rfm_precompute_free(C.byref(self.cd), C.byref(g.params), g.rfmstruct)
+            self.lib.bcstruct_free(C.byref(g.bcstruct))
+            self._rfm = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -14,13 +14,14 @@
 
 typedef struct {
   commondata_struct commondata;
-  griddata_struct griddata[MAXNUMGRIDS];
+  griddata_struct *griddata;  // malloc'd as in main(); griddata_free() releases it
 } ref_sim;
 
 ref_sim *ref_create(const int Nx0, const int Nx1, const int Nx2, const double grid_physical_size, const double sinhw,
                     const double m1, const double z1, const double m2, const double z2, const double cfl,
                     const int outer_bc_extrapolation) {
   ref_sim *s = (ref_sim *)calloc(1, sizeof(ref_sim));
+  s->griddata = (griddata_struct *)calloc(MAXNUMGRIDS, sizeof(griddata_struct));
   commondata_struct_set_to_default(&s->commondata);
   s->commondata.BH1_mass = m1;
   s->commondata.BH1_posn_z = z1;
