@@ -163,8 +163,13 @@ def main():
     ap.add_argument("--mode", type=int, default=1, help="0: reference stage order; 1: fused stages")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--nxx", default=None, help="override the grid, e.g. 256,64,32 (profiling only)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    global NXX
+    if args.nxx:
+        NXX = tuple(int(x) for x in args.nxx.split(","))
     if args.impl == "reference":
         return run_reference(args)
 
@@ -235,7 +240,7 @@ def main():
     achieved = bytes_launch / (kstats["ms_per_launch"] * 1e-3) / 1e9
 
     # ---------------- end-to-end through the public API with host buffers
-    e2e = run_e2e(grid, args, y0)
+    e2e = None if args.no_e2e else run_e2e(grid, args, y0)
     grid.free_stepper()
 
     if rank == 0:
@@ -249,7 +254,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (Brill-Lindquist initial data, seeded)",
-            "config": {"workload": "BSSN RK4, SinhSpherical 256x64x64 (+3 ghosts), AMPL=10, SINHW=0.2, FP64, "
+            "config": {"workload": f"BSSN RK4, SinhSpherical {NXX[0]}x{NXX[1]}x{NXX[2]} (+3 ghosts), AMPL=10, SINHW=0.2, FP64, "
                                    "KO, radiation BCs, H-constraint L2 every 20 steps",
                        "interior_points": pts, "mode": "fused stages" if args.mode == 1 else "reference stage order",
                        "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",

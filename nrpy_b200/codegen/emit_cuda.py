@@ -228,7 +228,7 @@ class PointKernel:
 
     def _ensure(self, expr: sp.Expr) -> None:
         for s in sorted(expr.free_symbols, key=lambda x: x.name):
-            if s.name.startswith("_cse"):
+            if s.name.startswith("_"):
                 continue
             if parse_deriv(s.name) and parse_deriv(s.name)[1] == "upD":
                 self._ensure_upwind()
@@ -244,18 +244,246 @@ class PointKernel:
             self.lines.append(f"const bool Upwind{i} = ({self.printer._print(e)}) > T(0.0);")
 
     # ---- driver -------------------------------------------------------------------
+    def _chain(self, name: str, expr: sp.Expr, order_of) -> List[Tuple[str, sp.Expr]]:
+        """Split a long sum into a chain of partial sums, terms ordered by when their
+        operands become available, so that each term's operands can die early."""
+        if not expr.is_Add or len(expr.args) <= 3:
+            return [(name, expr)]
+        terms = sorted(expr.args, key=lambda t: max([order_of(x) for x in t.free_symbols] + [-1]))
+        out: List[Tuple[str, sp.Expr]] = []
+        acc = sp.Add(terms[0], terms[1], evaluate=False)
+        for j, t in enumerate(terms[2:]):
+            nm = f"{name}_p{j}"
+            out.append((nm, acc))
+            acc = sp.Add(sp.Symbol(nm), t, evaluate=False)
+        out.append((name, acc))
+        return out
+
     def build(self, outputs: Sequence[Tuple[str, sp.Expr]], upwind_vec=None) -> str:
         self.upwind_vec = upwind_vec
         exprs = [sp.sympify(e) for _, e in outputs]
         syms = (sp.Symbol(f"_cse{i}") for i in range(10**7))
         repl, reduced = sp.cse(exprs, symbols=syms, order="none")
-        for s, e in repl:
+        pos = {s.name: i for i, (s, _) in enumerate(repl)}
+
+        def order_of(x):
+            return pos.get(x.name, -1)
+
+        stmts: List[Tuple[str, sp.Expr, bool]] = []  # (name, expr, is_output)
+        for sym, e in repl:
+            stmts += [(n, x, False) for n, x in self._chain(sym.name, e, order_of)]
+        for k, ((lhs, _), e) in enumerate(zip(outputs, reduced)):
+            chain = self._chain(f"_out{k}", e, order_of)
+            stmts += [(n, x, False) for n, x in chain[:-1]]
+            stmts.append((lhs, chain[-1][1], True))
+        # Leaf definitions are created lazily in first-use order (their "natural" slots).
+        nodes: List[Tuple[str, str]] = []  # (defined name or "", code line)
+        for name, e, is_out in stmts:
             self._ensure(e)
-            self.lines.append(f"const T {s.name} = {self.printer._print(e)};")
-        for (lhs, _), e in zip(outputs, reduced):
-            self._ensure(e)
-            self.lines.append(f"{lhs} = {self.printer._print(e)};")
+            self.lines.append(f"{name} = {self.printer._print(e)};" if is_out
+                              else f"const T {name} = {self.printer._print(e)};")
+        self.lines = schedule_lines(self.lines)
         return "\n".join("  " + ln for ln in self.lines)
+
+
+_DEF_RE = re.compile(r"\s*const (?:T|double|bool) (\w+) =")
+_TOK_RE = re.compile(r"[A-Za-z_]\w*")
+
+
+def schedule_lines(lines: List[str]) -> List[str]:
+    """Reorder straight-line statements to keep few values live (greedy list scheduling).
+
+    Among statements whose operands are all available, pick the one that ends the most
+    live ranges net of the value it creates; ties keep the original order.
+    """
+    defs: Dict[str, int] = {}
+    for i, ln in enumerate(lines):
+        m = _DEF_RE.match(ln)
+        if m:
+            defs[m.group(1)] = i
+    deps: List[List[int]] = []
+    users: List[List[int]] = [[] for _ in lines]
+    for i, ln in enumerate(lines):
+        body = ln.split("=", 1)[1]
+        ds = sorted({defs[t] for t in _TOK_RE.findall(body) if t in defs and defs[t] != i})
+        deps.append(ds)
+        for d in ds:
+            users[d].append(i)
+    remaining = [len(u) for u in users]
+    npend = [len(d) for d in deps]
+    is_def = [1 if _DEF_RE.match(ln) else 0 for ln in lines]
+    ready = {i for i in range(len(lines)) if npend[i] == 0}
+    order: List[int] = []
+    while ready:
+        best, bscore = -1, None
+        for s in ready:
+            kill = 0
+            for d in deps[s]:
+                if remaining[d] == 1:
+                    kill += 1
+            score = (kill - is_def[s], -s)
+            if bscore is None or score > bscore:
+                bscore, best = score, s
+        ready.remove(best)
+        order.append(best)
+        for d in deps[best]:
+            remaining[d] -= 1
+        for u in users[best]:
+            npend[u] -= 1
+            if npend[u] == 0:
+                ready.add(u)
+    if len(order) != len(lines):
+        raise RuntimeError("statement dependency cycle")
+    return [lines[i] for i in order]
+
+
+def dfs_order(lines: List[str]) -> List[str]:
+    """Topological order that completes one output at a time (post-order DFS from each
+    output in turn), so values shared by later outputs are the only long-lived ones."""
+    defs: Dict[str, int] = {}
+    for i, ln in enumerate(lines):
+        m = _DEF_RE.match(ln)
+        if m:
+            defs[m.group(1)] = i
+    deps = []
+    for i, ln in enumerate(lines):
+        body = ln.split("=", 1)[1]
+        deps.append([defs[t] for t in dict.fromkeys(_TOK_RE.findall(body)) if t in defs and defs[t] != i])
+    done = [False] * len(lines)
+    order: List[int] = []
+
+    def visit(root: int) -> None:
+        stack = [(root, 0)]
+        while stack:
+            node, k = stack.pop()
+            if done[node]:
+                continue
+            if k < len(deps[node]):
+                stack.append((node, k + 1))
+                d = deps[node][k]
+                if not done[d]:
+                    stack.append((d, 0))
+            else:
+                done[node] = True
+                order.append(node)
+
+    for i, ln in enumerate(lines):
+        if not _DEF_RE.match(ln):
+            visit(i)
+    for i in range(len(lines)):
+        if not done[i]:
+            visit(i)
+    return [lines[i] for i in order]
+
+
+def _parse(lines: List[str]):
+    """(defined name or None, type or None, rhs text, is_output) per statement."""
+    out = []
+    for ln in lines:
+        m = re.match(r"\s*const (T|double|bool) (\w+) = (.*);\s*$", ln)
+        if m:
+            out.append((m.group(2), m.group(1), m.group(3), False))
+        else:
+            lhs, rhs = ln.split("=", 1)
+            out.append((lhs.strip(), None, rhs.strip().rstrip(";"), True))
+    return out
+
+
+def _is_remat(ty: str, rhs: str, remat: Dict[str, str]) -> bool:
+    if ty == "double" and rhs.startswith("LD("):
+        return True
+    if ty == "T" and (rhs.startswith("T(RFM(") or rhs.startswith("T(PARAM(") or rhs.startswith("T(LDAUX(")):
+        return True
+    m = re.fullmatch(r"T\((v_\w+)\)", rhs)
+    return bool(m and m.group(1) in remat)
+
+
+def allocate_values(lines: List[str], reg_capacity: int) -> Tuple[List[str], int]:
+    """Keep at most `reg_capacity` values in registers at any statement.
+
+    Linear scan over live intervals (Poletto-Sarkar): when too many values are live, the
+    one whose interval ends last leaves the register set. Values that are plain loads
+    (stencil points, rfm arrays, parameters) are re-read at each use instead; all others
+    are stored once to a per-thread shared-memory slot, SMEM(k), and read from it at each
+    use (the slot array is volatile, so the compiler cannot keep the value in a register).
+    Returns the rewritten statements and the number of shared-memory slots.
+    """
+    st = _parse(lines)
+    n = len(st)
+    idx = {name: i for i, (name, ty, _, is_out) in enumerate(st) if not is_out}
+    last = {}
+    for i, (_, _, rhs, _) in enumerate(st):
+        for t in _TOK_RE.findall(rhs):
+            if t in idx:
+                last[t] = i
+    remat: Dict[str, str] = {}
+    for name, ty, rhs, is_out in st:
+        if not is_out and _is_remat(ty, rhs, remat):
+            remat[name] = rhs
+    # intervals of values that need storage (bools stay in registers: predicates)
+    iv = [(idx[v], last.get(v, idx[v]), v) for v in idx if st[idx[v]][1] != "bool"]
+    iv.sort()
+    active: List[Tuple[int, str]] = []  # (end, name) of values in registers
+    spilled: Dict[str, bool] = {}
+    import bisect
+
+    for start, end, v in iv:
+        active = [(e, a) for e, a in active if e > start]  # intervals ending at start are done
+        bisect.insort(active, (end, v))
+        if len(active) > reg_capacity:
+            e, victim = active.pop()  # furthest end
+            spilled[victim] = True
+    # shared-memory slots for spilled, non-rematerializable values (interval colouring)
+    slot_of: Dict[str, int] = {}
+    free: List[int] = []
+    busy: List[Tuple[int, int]] = []  # (end, slot)
+    nslots = 0
+    for start, end, v in iv:
+        if v not in spilled or v in remat:
+            continue
+        keep = []
+        for e, k in busy:
+            if e < start:
+                free.append(k)
+            else:
+                keep.append((e, k))
+        busy = keep
+        if free:
+            free.sort()
+            k = free.pop(0)
+        else:
+            k = nslots
+            nslots += 1
+        slot_of[v] = k
+        busy.append((end, k))
+
+    def rewrite(rhs: str) -> str:
+        def sub(m):
+            t = m.group(0)
+            if t in spilled:
+                if t in remat:
+                    r = remat[t]
+                    inner = re.fullmatch(r"T\((v_\w+)\)", r)
+                    if inner and inner.group(1) in remat:
+                        return f"T({remat[inner.group(1)]})"
+                    return f"({r})"
+                return f"SMEM({slot_of[t]})"
+            return t
+
+        return _TOK_RE.sub(sub, rhs)
+
+    out: List[str] = []
+    for name, ty, rhs, is_out in st:
+        r = rewrite(rhs)
+        if is_out:
+            out.append(f"{name} = {r};")
+        elif name in spilled and name in remat:
+            continue  # re-read at each use
+        elif name in slot_of:
+            out.append(f"SMEM({slot_of[name]}) = {r};")
+        else:
+            out.append(f"const {ty} {name} = {r};")
+    return out, nslots
 
 
 def emit_point_function(
@@ -264,13 +492,22 @@ def emit_point_function(
     upwind_vec=None,
     symmetry_axes: str = "",
     comment: str = "",
+    reg_capacity: int = 0,
 ) -> Tuple[str, Dict[str, int]]:
+    """Emit `fname` and the constant `fname_SMEM_SLOTS`. With reg_capacity > 0 the values
+    beyond that many live doubles go to shared-memory slots (SMEM(k), provided by the
+    caller through the `sm` argument: slot k of this thread)."""
     pk = PointKernel(symmetry_axes)
-    body = pk.build(outputs, upwind_vec)
+    pk.build(outputs, upwind_vec)
+    lines, nslots = (allocate_values(dfs_order(pk.lines), reg_capacity) if reg_capacity > 0 else (pk.lines, 0))
+    body = "\n".join("  " + ln for ln in lines)
     head = f"// {comment}\n" if comment else ""
     code = (
-        f"{head}template <typename T, typename TF, typename Ctx>\n"
-        f"__device__ __forceinline__ void {fname}(const Ctx &ctx, T *__restrict__ out) {{\n"
-        f"{body}\n}}\n"
+        f"{head}constexpr int {fname}_SMEM_SLOTS = {nslots};\n"
+        f"template <typename T, typename TF, typename Ctx>\n"
+        f"__device__ __forceinline__ void {fname}(const Ctx &ctx, T *__restrict__ out, volatile T *sm) {{\n"
+        f"  (void)sm;\n{body}\n}}\n"
     )
-    return code, dict(pk.stats)
+    stats = dict(pk.stats)
+    stats["smem_slots"] = nslots
+    return code, stats

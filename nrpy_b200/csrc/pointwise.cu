@@ -6,9 +6,14 @@
 // Layout: gf-major IDX4(gf,i0,i1,i2) = i0 + N0*(i1 + N1*(i2 + N2*gf)). One thread per
 // interior point; a warp spans 32 consecutive i0, so each stencil load of a warp touches
 // one or two contiguous 256-byte segments that neighbouring warps reuse from L1/L2.
+#include <type_traits>
+
 #include "bssn_common.cuh"
 
 namespace bssn {
+
+// Interior block geometry: 32 points along i0 x 4 along i1, one i2 plane per blockIdx.z.
+constexpr int BX = 32, BY = 4;
 
 template <typename T>
 __device__ __forceinline__ T ipow(T x, int n) {
@@ -51,6 +56,8 @@ struct RegCtx {
 #define rfm_f1_D1 f1_D1
 #define rfm_f1_DD11 f1_DD11
 #define PARAM(name) ctx.name
+// Per-thread shared-memory slot k (the kernel passes `sm` already offset by its thread).
+#define SMEM(k) sm[(k) * (BX * BY)]
 #define invdxx0 ctx.invdxx0
 #define invdxx1 ctx.invdxx1
 #define invdxx2 ctx.invdxx2
@@ -62,12 +69,27 @@ struct RegCtx {
 #undef invdxx1
 #undef invdxx2
 
-#define DISPATCH_POINT(NAME, V, T, TF, CTX, OUT)                            \
-  do {                                                                      \
-    if constexpr (V == SPH_3D) NAME##_sph_3d<T, TF>(CTX, OUT);              \
-    else if constexpr (V == SPH_AXI) NAME##_sph_axi<T, TF>(CTX, OUT);       \
-    else if constexpr (V == SINH_3D) NAME##_sinh_3d<T, TF>(CTX, OUT);       \
-    else NAME##_sinh_axi<T, TF>(CTX, OUT);                                  \
+// Output-group traits of the generated variants: RicciGroup<V,G> / RhsGroup<V,G> expose
+// N (outputs), GF[] (their gridfunction indices), SLOTS (per-thread shared-memory slots of
+// the spilled values) and eval().
+template <Variant V, int G>
+using RicciG = std::conditional_t<
+    V == SPH_3D, RicciGroup_sph_3d<G>,
+    std::conditional_t<V == SPH_AXI, RicciGroup_sph_axi<G>,
+                       std::conditional_t<V == SINH_3D, RicciGroup_sinh_3d<G>, RicciGroup_sinh_axi<G>>>>;
+template <Variant V, int G>
+using RhsG = std::conditional_t<
+    V == SPH_3D, RhsGroup_sph_3d<G>,
+    std::conditional_t<V == SPH_AXI, RhsGroup_sph_axi<G>,
+                       std::conditional_t<V == SINH_3D, RhsGroup_sinh_3d<G>, RhsGroup_sinh_axi<G>>>>;
+constexpr int kRicciGroups = 3, kRhsGroups = 3;
+
+#define DISPATCH_POINT(NAME, V, T, TF, CTX, OUT)                                  \
+  do {                                                                            \
+    if constexpr (V == SPH_3D) NAME##_sph_3d<T, TF>(CTX, OUT, nullptr);           \
+    else if constexpr (V == SPH_AXI) NAME##_sph_axi<T, TF>(CTX, OUT, nullptr);    \
+    else if constexpr (V == SINH_3D) NAME##_sinh_3d<T, TF>(CTX, OUT, nullptr);    \
+    else NAME##_sinh_axi<T, TF>(CTX, OUT, nullptr);                               \
   } while (0)
 
 __device__ __forceinline__ PointCtx make_ctx(const GridDims &g, const RfmArrays &rfm, const double *in,
@@ -91,8 +113,6 @@ __device__ __forceinline__ PointCtx make_ctx(const GridDims &g, const RfmArrays 
   return c;
 }
 
-// Interior block geometry: 32 points along i0 x 4 along i1, one i2 plane per blockIdx.z.
-constexpr int BX = 32, BY = 4;
 static dim3 interior_grid(const GridDims &g) {
   const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
   return dim3((n0 + BX - 1) / BX, (n1 + BY - 1) / BY, n2);
@@ -104,32 +124,42 @@ static dim3 interior_grid(const GridDims &g) {
   const int i2 = NGHOSTS + blockIdx.z;                    \
   if (i0 >= g.N0 - NGHOSTS || i1 >= g.N1 - NGHOSTS) return;
 
-template <Variant V>
-__global__ void __launch_bounds__(BX *BY, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
-                                                       const double *__restrict__ in, double *__restrict__ aux) {
-  INTERIOR_INDEX_OR_RETURN(g);
-  const PointCtx ctx = make_ctx(g, rfm, in, nullptr, i0, i1, i2);
-  double out[6];
-  DISPATCH_POINT(ricci_point, V, double, double, ctx, out);
-  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
-#pragma unroll
-  for (int k = 0; k < 6; k++) aux[idx + k * g.ntot] = out[k];
+template <typename T>
+__device__ __forceinline__ volatile T *thread_slots() {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + BX * threadIdx.y);
 }
 
-template <Variant V, typename T>
+template <Variant V, int G>
+__global__ void __launch_bounds__(BX *BY, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
+                                                          const double *__restrict__ in, double *__restrict__ aux) {
+  using Grp = RicciG<V, G>;
+  volatile double *sm = thread_slots<double>();
+  INTERIOR_INDEX_OR_RETURN(g);
+  const PointCtx ctx = make_ctx(g, rfm, in, nullptr, i0, i1, i2);
+  double out[Grp::N];
+  Grp::template eval<double, double>(ctx, out, sm);
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+#pragma unroll
+  for (int k = 0; k < Grp::N; k++) aux[idx + Grp::GF(k) * g.ntot] = out[k];
+}
+
+template <Variant V, typename T, int G>
 __global__ void __launch_bounds__(BX *BY, 1) rhs_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
-                                                     const double *__restrict__ aux, const double *__restrict__ in,
-                                                     double *__restrict__ rhs) {
+                                                        const double *__restrict__ aux, const double *__restrict__ in,
+                                                        double *__restrict__ rhs) {
+  using Grp = RhsG<V, G>;
+  volatile T *sm = thread_slots<T>();
   INTERIOR_INDEX_OR_RETURN(g);
   PointCtx ctx = make_ctx(g, rfm, in, aux, i0, i1, i2);
   ctx.eta = pp.eta;
   ctx.KreissOliger_strength_gauge = pp.ko_gauge;
   ctx.KreissOliger_strength_nongauge = pp.ko_nongauge;
-  T out[NUM_EVOL_GFS];
-  DISPATCH_POINT(rhs_point, V, T, double, ctx, out);
+  T out[Grp::N];
+  Grp::template eval<T, double>(ctx, out, sm);
   const int idx = i0 + g.s1 * i1 + g.s2 * i2;
 #pragma unroll
-  for (int k = 0; k < NUM_EVOL_GFS; k++) rhs[idx + k * g.ntot] = double(out[k]);
+  for (int k = 0; k < Grp::N; k++) rhs[idx + Grp::GF(k) * g.ntot] = double(out[k]);
 }
 
 template <Variant V>
@@ -215,31 +245,50 @@ __device__ __forceinline__ void rk_and_project_point(const GridDims &g, const Rf
   for (int k = 0; k < NUM_EVOL_GFS; k++) b.kout[idx + (size_t)k * g.ntot] = o[k];
 }
 
-// RHS at an interior point, then in registers the RK4 stage update and the detgammabar
-// projection of the stage output. The raw RHS is also stored to `krhs` on the interior
-// shell (the layer next to each face), where the outer radiation condition reads it.
-template <Variant V, typename T, int STAGE>
+// One output group of the RHS at an interior point, then in registers the RK4 stage update
+// of that group's gridfunctions; the group holding hDD also applies the detgammabar
+// projection to the new hDD. The raw RHS is also stored to `krhs` on the interior shell
+// (the layer next to each face), where the outer radiation condition reads it.
+template <Variant V, typename T, int STAGE, int G>
 __global__ void __launch_bounds__(BX *BY, 1) rhs_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
-                                                           const double *__restrict__ aux, const StageBuffers b,
-                                                           double *__restrict__ krhs, const double dt) {
+                                                              const double *__restrict__ aux, const StageBuffers b,
+                                                              double *__restrict__ krhs, const double dt) {
+  using Grp = RhsG<V, G>;
+  volatile T *sm = thread_slots<T>();
   INTERIOR_INDEX_OR_RETURN(g);
   PointCtx ctx = make_ctx(g, rfm, b.kin, aux, i0, i1, i2);
   ctx.eta = pp.eta;
   ctx.KreissOliger_strength_gauge = pp.ko_gauge;
   ctx.KreissOliger_strength_nongauge = pp.ko_nongauge;
-  T kt[NUM_EVOL_GFS];
-  DISPATCH_POINT(rhs_point, V, T, double, ctx, kt);
-  double kk[NUM_EVOL_GFS];
-#pragma unroll
-  for (int k = 0; k < NUM_EVOL_GFS; k++) kk[k] = double(kt[k]);
+  T kt[Grp::N];
+  Grp::template eval<T, double>(ctx, kt, sm);
   const int idx = i0 + g.s1 * i1 + g.s2 * i2;
   const bool shell = (i0 == NGHOSTS) | (i0 == g.N0 - NGHOSTS - 1) | (i1 == NGHOSTS) | (i1 == g.N1 - NGHOSTS - 1) |
                      (i2 == NGHOSTS) | (i2 == g.N2 - NGHOSTS - 1);
-  if (shell) {
+  double o[NUM_EVOL_GFS];  // indexed by gridfunction; only this group's entries are used
+  constexpr bool has_h = [] {
+    int n = 0;
+    for (int k = 0; k < Grp::N; k++) n += (Grp::GF(k) >= HDD00GF && Grp::GF(k) <= HDD22GF);
+    return n == 6;
+  }();
 #pragma unroll
-    for (int k = 0; k < NUM_EVOL_GFS; k++) krhs[idx + (size_t)k * g.ntot] = kk[k];
+  for (int k = 0; k < Grp::N; k++) {
+    const double kv = double(kt[k]);
+    const size_t a = idx + (size_t)Grp::GF(k) * g.ntot;
+    if (shell) krhs[a] = kv;
+    double run = (STAGE == 1) ? 0.0 : b.run[a];
+    rk_update<STAGE>(kv, b.y[a], run, o[Grp::GF(k)], dt);
+    if (STAGE != 4) b.run[a] = run;
   }
-  rk_and_project_point<V, STAGE>(g, rfm, b, idx, i0, i1, kk, dt);
+  if constexpr (has_h) {
+    RegCtx rc{o, i0, i1, rfm};
+    double h[6];
+    DISPATCH_POINT(enforce_point, V, double, double, rc, h);
+#pragma unroll
+    for (int k = 0; k < 6; k++) o[HDD00GF + k] = h[k];
+  }
+#pragma unroll
+  for (int k = 0; k < Grp::N; k++) b.kout[idx + (size_t)Grp::GF(k) * g.ntot] = o[Grp::GF(k)];
 }
 
 // RK update plus projection of listed boundary points whose RHS is already in krhs.
@@ -258,9 +307,6 @@ __global__ void rk_points_kernel(const GridDims g, const RfmArrays rfm, const St
 }
 
 // ---------------------------------------------------------------- launchers
-template <template <Variant> class K>
-struct Dummy {};
-
 #define VARIANT_SWITCH(v, CALL)                 \
   switch (v) {                                  \
     case SPH_3D: { constexpr Variant VV = SPH_3D; CALL; } break;   \
@@ -274,22 +320,70 @@ static bool empty_interior(const GridDims &g) {
   return g.N0 <= 2 * NGHOSTS || g.N1 <= 2 * NGHOSTS || g.N2 <= 2 * NGHOSTS;
 }
 
-int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
-  if (empty_interior(g)) return BSSN_B200_OK;
-  VARIANT_SWITCH(v, (ricci_kernel<VV><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, in, aux)));
+// Dynamic shared memory of a group kernel: SLOTS values of type T per thread.
+template <typename Grp, typename T>
+constexpr size_t slot_bytes() {
+  return (size_t)Grp::SLOTS * BX * BY * sizeof(T);
+}
+
+template <typename KernelPtr>
+static int set_smem(KernelPtr k, size_t bytes) {
+  if (bytes > 48 * 1024) BSSN_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return BSSN_B200_OK;
+}
+
+template <Variant V, int G>
+static int launch_ricci_group(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
+  using Grp = RicciG<V, G>;
+  constexpr size_t sb = slot_bytes<Grp, double>();
+  BSSN_TRY(set_smem(ricci_kernel<V, G>, sb));
+  ricci_kernel<V, G><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, in, aux);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
+}
+
+template <Variant V>
+static int launch_ricci_v(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
+  static_assert(kRicciGroups == 3, "group count");
+  BSSN_TRY((launch_ricci_group<V, 0>(g, rfm, in, aux, s)));
+  BSSN_TRY((launch_ricci_group<V, 1>(g, rfm, in, aux, s)));
+  return launch_ricci_group<V, 2>(g, rfm, in, aux, s);
+}
+
+int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
+  if (empty_interior(g)) return BSSN_B200_OK;
+  VARIANT_SWITCH(v, return launch_ricci_v<VV>(g, rfm, in, aux, s));
+  return BSSN_B200_OK;
+}
+
+template <Variant V, typename T, int G>
+static int launch_rhs_group(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp, const double *aux,
+                            const double *in, double *rhs, cudaStream_t s) {
+  using Grp = RhsG<V, G>;
+  constexpr size_t sb = slot_bytes<Grp, T>();
+  BSSN_TRY(set_smem(rhs_kernel<V, T, G>, sb));
+  rhs_kernel<V, T, G><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, pp, aux, in, rhs);
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+template <Variant V, typename T>
+static int launch_rhs_v(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp, const double *aux,
+                        const double *in, double *rhs, cudaStream_t s) {
+  static_assert(kRhsGroups == 3, "group count");
+  BSSN_TRY((launch_rhs_group<V, T, 0>(g, rfm, pp, aux, in, rhs, s)));
+  BSSN_TRY((launch_rhs_group<V, T, 1>(g, rfm, pp, aux, in, rhs, s)));
+  return launch_rhs_group<V, T, 2>(g, rfm, pp, aux, in, rhs, s);
 }
 
 int launch_rhs(Variant v, bool mixed, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
                const double *aux, const double *in, double *rhs, cudaStream_t s) {
   if (empty_interior(g)) return BSSN_B200_OK;
   if (mixed) {
-    VARIANT_SWITCH(v, (rhs_kernel<VV, float><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, pp, aux, in, rhs)));
+    VARIANT_SWITCH(v, return (launch_rhs_v<VV, float>(g, rfm, pp, aux, in, rhs, s)));
   } else {
-    VARIANT_SWITCH(v, (rhs_kernel<VV, double><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, pp, aux, in, rhs)));
+    VARIANT_SWITCH(v, return (launch_rhs_v<VV, double>(g, rfm, pp, aux, in, rhs, s)));
   }
-  BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
 
@@ -316,15 +410,34 @@ int launch_enforce(Variant v, const GridDims &g, const RfmArrays &rfm, double *g
   return BSSN_B200_OK;
 }
 
+template <Variant V, typename T, int STAGE, int G>
+static int launch_fused_group(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp, const double *aux,
+                              const StageBuffers &b, double *krhs, double dt, cudaStream_t s) {
+  using Grp = RhsG<V, G>;
+  constexpr size_t sb = slot_bytes<Grp, T>();
+  BSSN_TRY(set_smem(rhs_fused_kernel<V, T, STAGE, G>, sb));
+  rhs_fused_kernel<V, T, STAGE, G><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, pp, aux, b, krhs, dt);
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+template <Variant V, typename T, int STAGE>
+static int launch_fused_stage_groups(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp, const double *aux,
+                                     const StageBuffers &b, double *krhs, double dt, cudaStream_t s) {
+  static_assert(kRhsGroups == 3, "group count");
+  BSSN_TRY((launch_fused_group<V, T, STAGE, 0>(g, rfm, pp, aux, b, krhs, dt, s)));
+  BSSN_TRY((launch_fused_group<V, T, STAGE, 1>(g, rfm, pp, aux, b, krhs, dt, s)));
+  return launch_fused_group<V, T, STAGE, 2>(g, rfm, pp, aux, b, krhs, dt, s);
+}
+
 template <Variant V, typename T>
-static void launch_fused_typed(int stage, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
-                               const double *aux, const StageBuffers &b, double *krhs, double dt, cudaStream_t s) {
-  const dim3 grid = interior_grid(g), block(BX, BY);
+static int launch_fused_typed(int stage, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
+                              const double *aux, const StageBuffers &b, double *krhs, double dt, cudaStream_t s) {
   switch (stage) {
-    case 1: rhs_fused_kernel<V, T, 1><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
-    case 2: rhs_fused_kernel<V, T, 2><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
-    case 3: rhs_fused_kernel<V, T, 3><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
-    default: rhs_fused_kernel<V, T, 4><<<grid, block, 0, s>>>(g, rfm, pp, aux, b, krhs, dt); break;
+    case 1: return launch_fused_stage_groups<V, T, 1>(g, rfm, pp, aux, b, krhs, dt, s);
+    case 2: return launch_fused_stage_groups<V, T, 2>(g, rfm, pp, aux, b, krhs, dt, s);
+    case 3: return launch_fused_stage_groups<V, T, 3>(g, rfm, pp, aux, b, krhs, dt, s);
+    default: return launch_fused_stage_groups<V, T, 4>(g, rfm, pp, aux, b, krhs, dt, s);
   }
 }
 
@@ -337,11 +450,10 @@ int launch_rhs_fused_stage(Variant v, bool mixed, int stage, double dt, const Gr
   }
   if (empty_interior(g)) return BSSN_B200_OK;
   if (mixed) {
-    VARIANT_SWITCH(v, (launch_fused_typed<VV, float>(stage, g, rfm, pp, aux, b, krhs, dt, s)));
+    VARIANT_SWITCH(v, return (launch_fused_typed<VV, float>(stage, g, rfm, pp, aux, b, krhs, dt, s)));
   } else {
-    VARIANT_SWITCH(v, (launch_fused_typed<VV, double>(stage, g, rfm, pp, aux, b, krhs, dt, s)));
+    VARIANT_SWITCH(v, return (launch_fused_typed<VV, double>(stage, g, rfm, pp, aux, b, krhs, dt, s)));
   }
-  BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
 
