@@ -57,6 +57,8 @@ int bl_initial_data(const commondata_struct *cd, const params_struct *p, REAL *x
 int constraint_integrals(const params_struct *p, const RfmArrays &rfm, const double *diag, double *scratch,
                          double out[4], cudaStream_t s);
 size_t constraint_integrals_scratch_doubles();
+int constraint_integrals_noalloc(const params_struct *p, const RfmArrays &rfm, const double *diag, double out[4],
+                                 cudaStream_t s);
 // MoL (mol.cu)
 int mol_step(commondata_struct *cd, griddata_struct *gd, int mode, int mixed, cudaStream_t s);
 int fused_interior_stage(const commondata_struct *cd, griddata_struct *gd, int grid, int stage, int mixed,
@@ -299,6 +301,15 @@ int bssn_b200_constraint_integrals(const params_struct *params, const rfm_struct
     if (!scratch[dev]) BSSN_CUDA_TRY(cudaMalloc(&scratch[dev], sizeof(double) * constraint_integrals_scratch_doubles()));
   }
   return constraint_integrals(params, rfm_arrays(rfmstruct), diagnostic_gfs, scratch[dev], out, (cudaStream_t)stream);
+}
+
+int bssn_b200_constraint_integrals_noalloc(const params_struct *params, const rfm_struct *rfmstruct,
+                                           const REAL *diagnostic_gfs, double out[4], void *stream) {
+  BSSN_TRY(check_ptr(params, "params"));
+  BSSN_TRY(check_ptr(rfmstruct, "rfmstruct"));
+  BSSN_TRY(check_ptr(diagnostic_gfs, "diagnostic_gfs"));
+  BSSN_TRY(check_ptr(out, "out"));
+  return constraint_integrals_noalloc(params, rfm_arrays(rfmstruct), diagnostic_gfs, out, (cudaStream_t)stream);
 }
 
 int bssn_b200_mol_step(commondata_struct *commondata, griddata_struct *griddata, int mode, int mixed, void *stream) {

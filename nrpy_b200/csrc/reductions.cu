@@ -6,6 +6,8 @@
 // precompute arrays. Each block reduces a fixed slice of the interior with warp shuffles
 // into a partial; a single block then adds the partials in a fixed order, so the result
 // does not depend on scheduling.
+#include <mutex>
+
 #include "bssn_common.cuh"
 
 namespace bssn {
@@ -88,5 +90,118 @@ int constraint_integrals(const params_struct *p, const RfmArrays &rfm, const dou
 }
 
 size_t constraint_integrals_scratch_doubles() { return (size_t)kRedBlocks * kRedVals + kRedVals; }
+
+// ---------------------------------------------------------------- allocation-free variant
+// Same integrals, for callers that must not allocate device memory: code running inside
+// a host framework that owns every allocation (a memory pool or arena that a foreign
+// cudaMalloc would bypass), code driven from a CUDA-graph-capture region, or embedded
+// hosts that forbid allocation after start-up. The partial sums live in a file-scope
+// __device__ array instead: one partial per block of kNoAllocPtsPerBlock interior points,
+// at most kNoAllocMaxBlocks blocks, i.e. grids of up to
+// kNoAllocMaxBlocks * kNoAllocPtsPerBlock = 33,554,432 interior points (512 KiB + 32 B of
+// device memory, held by every GPU that loads the library until the process exits).
+constexpr int kNoAllocThreads = 256;
+constexpr int kNoAllocPtsPerThread = 8;
+constexpr int kNoAllocPtsPerBlock = kNoAllocThreads * kNoAllocPtsPerThread;
+constexpr int kNoAllocMaxBlocks = 16384;
+static __device__ __align__(256) double g_noalloc_scratch[(size_t)kNoAllocMaxBlocks * kRedVals + kRedVals];
+
+// Block b sums interior points [b*kNoAllocPtsPerBlock, (b+1)*kNoAllocPtsPerBlock) in a fixed
+// order and writes its own partial; nothing accumulates across blocks or calls, so no entry
+// has to start at zero.
+__global__ void __launch_bounds__(kNoAllocThreads) constraint_partials_blocked_kernel(
+    const GridDims g, const RfmArrays rfm, const double dvol, const double *__restrict__ diag,
+    double *__restrict__ partials) {
+  const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
+  const long long n = (long long)n0 * n1 * n2;
+  double acc[kRedVals] = {0.0, 0.0, 0.0, 0.0};
+  const long long base = (long long)blockIdx.x * kNoAllocPtsPerBlock;
+  for (int j = 0; j < kNoAllocPtsPerThread; j++) {
+    const long long t = base + (long long)j * kNoAllocThreads + threadIdx.x;
+    if (t >= n) break;
+    const int i0 = NGHOSTS + (int)(t % n0);
+    const long long q = t / n0;
+    const int i1 = NGHOSTS + (int)(q % n1);
+    const int i2 = NGHOSTS + (int)(q / n1);
+    const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+    const double f0 = rfm.f0[i0];
+    const double dV = fabs(rfm.f0_D0[i0] * f0 * f0 * rfm.f1[i1]) * dvol;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double f = diag[idx + (size_t)k * g.ntot];
+      acc[k] += f * f * dV;
+    }
+    acc[3] += dV;
+  }
+  __shared__ double sh[kRedVals][kNoAllocThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kRedVals; k++) {
+    const double w = warp_sum(acc[k]);
+    if (lane == 0) sh[k][warp] = w;
+  }
+  __syncthreads();
+  if (threadIdx.x < kRedVals) {
+    double sum = 0.0;
+    for (int w = 0; w < kNoAllocThreads / 32; w++) sum += sh[threadIdx.x][w];
+    partials[blockIdx.x * kRedVals + threadIdx.x] = sum;
+  }
+}
+
+long long constraint_integrals_noalloc_max_points() { return (long long)kNoAllocMaxBlocks * kNoAllocPtsPerBlock; }
+
+// Device address of g_noalloc_scratch, looked up once per device with that device current.
+static double *noalloc_scratch_address(int *rc) {
+  static std::mutex mu;
+  static double *addr[64] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+    set_error("no-alloc integrals: cudaGetDevice failed (%s)", cudaGetErrorString(e));
+    *rc = BSSN_B200_ECUDA;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    double *p = nullptr;
+    e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+      set_error("no-alloc integrals: cudaGetSymbolAddress failed on device %d (%s)", dev, cudaGetErrorString(e));
+      *rc = BSSN_B200_ECUDA;
+      return nullptr;
+    }
+    addr[dev] = p;
+  }
+  *rc = BSSN_B200_OK;
+  return addr[dev];
+}
+
+int constraint_integrals_noalloc(const params_struct *p, const RfmArrays &rfm, const double *diag, double out[4],
+                                 cudaStream_t s) {
+  const GridDims g = grid_dims(p);
+  if (g.N0 <= 2 * NGHOSTS || g.N1 <= 2 * NGHOSTS || g.N2 <= 2 * NGHOSTS) {
+    for (int k = 0; k < 4; k++) out[k] = 0.0;
+    return BSSN_B200_OK;
+  }
+  const long long n = (long long)(g.N0 - 2 * NGHOSTS) * (g.N1 - 2 * NGHOSTS) * (g.N2 - 2 * NGHOSTS);
+  if (n > constraint_integrals_noalloc_max_points()) {
+    set_error("no-alloc integrals: %lld interior points exceed the static scratch limit of %lld points", n,
+              constraint_integrals_noalloc_max_points());
+    return BSSN_B200_EINVAL;
+  }
+  int rc = BSSN_B200_OK;
+  double *scratch = noalloc_scratch_address(&rc);
+  if (rc != BSSN_B200_OK) return rc;
+  const int nblocks = (int)((n + kNoAllocPtsPerBlock - 1) / kNoAllocPtsPerBlock);
+  const double dvol = fabs(p->dxx0 * p->dxx1 * p->dxx2);
+  constraint_partials_blocked_kernel<<<nblocks, kNoAllocThreads, 0, s>>>(g, rfm, dvol, diag, scratch);
+  BSSN_LAUNCH_CHECK();
+  double *res = scratch + (size_t)kNoAllocMaxBlocks * kRedVals;
+  sum_partials_kernel<<<1, 32 * kRedVals, 0, s>>>(scratch, nblocks, res);
+  BSSN_LAUNCH_CHECK();
+  BSSN_CUDA_TRY(cudaMemcpyAsync(out, res, sizeof(double) * kRedVals, cudaMemcpyDeviceToHost, s));
+  BSSN_CUDA_TRY(cudaStreamSynchronize(s));
+  return BSSN_B200_OK;
+}
 
 }  // namespace bssn

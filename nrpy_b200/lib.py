@@ -162,6 +162,7 @@ SIGNATURES = [
     ("bssn_b200_enforce_detgammabar_equals_detgammahat", C.c_int, [PP, PRFM, PR, V]),
     ("bssn_b200_constraints_eval", C.c_int, [PCD, PP, PRFM, PR, PR, PR, V]),
     ("bssn_b200_constraint_integrals", C.c_int, [PP, PRFM, PR, C.POINTER(C.c_double), V]),
+    ("bssn_b200_constraint_integrals_noalloc", C.c_int, [PP, PRFM, PR, C.POINTER(C.c_double), V]),
     ("bssn_b200_mol_step", C.c_int, [PCD, PGD, C.c_int, C.c_int, V]),
     ("bssn_b200_stepper_create", C.c_int, [PCD, PGD, C.c_int, C.c_int, C.c_int, V, C.POINTER(V)]),
     ("bssn_b200_stepper_run", C.c_int, [V, C.c_int]),
