@@ -45,6 +45,20 @@ def bl_params(seed: int):
     return float(m1), float(z1), float(m2), float(z2)
 
 
+def aggregate(pts_local: int, steps: int, ms_local: float, dist=None, device="cpu"):
+    """Whole-job rate of N independent replicas: sum of the ranks' point updates divided by
+    the slowest rank's device time (max over ranks). Returns (value, max_ms)."""
+    if dist is None:
+        return pts_local * steps / (ms_local * 1e-3), ms_local
+    import torch
+
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    n = torch.tensor([float(pts_local) * steps], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(n.item()) / (float(t.item()) * 1e-3), float(t.item())
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -226,11 +240,7 @@ def main():
         stop.synchronize()
     launches = lib.bssn_b200_kernel_launches() - launches0
     ms = start.elapsed_time(stop)
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * pts * args.steps / (ms * 1e-3)
+    value, ms = aggregate(pts, args.steps, ms, dist, device="cuda")
     clocks = clk.summary()
 
     # ---------------- dominant kernel alone: fused interior RHS + RK update, per stage

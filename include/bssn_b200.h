@@ -313,6 +313,23 @@ int bssn_b200_stepper_destroy(bssn_b200_stepper *st);
 /* Number of kernel nodes in one replay of the stepper's graph. */
 int bssn_b200_stepper_kernel_nodes(const bssn_b200_stepper *st, unsigned long long *out);
 
+/* Batched evolutions: `nevo` independent grids (each set up through the entry points above:
+ * grid, rfm, bcstruct, storage, initial data; all of one coordinate system, full 3-D,
+ * radiation outer BCs; each with its own commondata: masses, dt, ...) advanced together.
+ * Each RK4 stage of the whole batch takes a fixed number of launches: persistent kernels
+ * (`blocks` CTAs of tile_bx x tile_by = 128 threads) walk one tile list over all grids.
+ * `steps_per_graph` RK4 steps are captured into a CUDA graph on `stream` (non-default);
+ * bssn_b200_batch_run replays it. Creation allocates the per-grid RHS shells and the
+ * device work lists; the caller's states are unchanged by it. */
+typedef struct bssn_b200_batch bssn_b200_batch;
+int bssn_b200_batch_create(int nevo, commondata_struct *const *commondatas, griddata_struct *const *griddatas,
+                           int tile_bx, int tile_by, int blocks, int steps_per_graph, void *stream,
+                           bssn_b200_batch **out);
+int bssn_b200_batch_run(bssn_b200_batch *batch, int graph_launches);
+int bssn_b200_batch_info(const bssn_b200_batch *batch, int *ntiles, int *nouter, int *ninner,
+                         unsigned long long *kernel_nodes);
+int bssn_b200_batch_destroy(bssn_b200_batch *batch);
+
 /* Instrumentation: kernels launched by this library since it was loaded (each graph replay
  * counts its kernel nodes), and a launch of only the interior RHS + RK-update + projection
  * kernel of RK4 stage `stage` (1..4) of grid 0, used to time the dominant kernel alone.

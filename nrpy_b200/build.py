@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libbssn_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["abi.cu", "setup.cu", "pointwise.cu", "boundary.cu", "mol.cu", "reductions.cu"]
+SOURCES = ["abi.cu", "setup.cu", "pointwise.cu", "boundary.cu", "mol.cu", "reductions.cu", "batch.cu"]
 
 
 def nvcc() -> str:

@@ -235,4 +235,73 @@ int launch_radiation_rk_bcs(Variant v, const GridDims &g, const params_struct *p
   return launch_inner_bcs(g, bc, b.kout, NUM_EVOL_GFS, nullptr, s);
 }
 
+// ---------------------------------------------------------------- batched evolutions
+// Radiation RHS of one ghost layer's pure outer points of every evolution (one thread per
+// point and gridfunction); reads the stage input and the RHS one layer in, writes krhs.
+__global__ void radiation_batched_kernel(const EvoDesc *__restrict__ descs, const BatchOuterPt *__restrict__ pts,
+                                         const int npts, const int stage) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * NUM_EVOL_GFS) return;
+  const int gf = t / npts;
+  const BatchOuterPt q = pts[t - gf * npts];
+  const EvoDesc &d = descs[q.evo];
+  double *kin, *kout;
+  stage_io(d, stage, kin, kout);
+  const RadialMap rm{d.radial_sinh, d.AMPL, d.SINHW};
+  const GridDims &g = d.g;
+  const outerpt_bc_struct p = q.p;
+  const int i0 = p.i0, i1 = p.i1, i2 = p.i2;
+  const int j0 = i0 + p.FACEX0, j1 = i1 + p.FACEX1, j2 = i2 + p.FACEX2;
+  double r, dx0dr, r_int, dx0dr_int;
+  rm.eval(d.xx0[i0], r, dx0dr);
+  rm.eval(d.xx0[j0], r_int, dx0dr_int);
+  const double *f = kin + (size_t)gf * g.ntot;
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+  const int idx_int = j0 + g.s1 * j1 + g.s2 * j2;
+  const double dfdr = dx0dr * fd1_x0(f, idx, fd1_offset(i0, p.FACEX0, g.N0), g.invdxx0);
+  const double dfdr_int = dx0dr_int * fd1_x0(f, idx_int, fd1_offset(j0, p.FACEX0, g.N0), g.invdxx0);
+  const double c = (gf == ALPHAGF) ? 1.41421356237310 : 1.0;
+  const double finf = (gf == ALPHAGF || gf == CFGF) ? 1.0 : 0.0;
+  double *rhs = d.krhs + (size_t)gf * g.ntot;
+  const double dtf_int = rhs[idx_int];
+  const double fv = f[idx], fv_int = f[idx_int];
+  const double out_int = -c * (dfdr_int + (fv_int - finf) / r_int);
+  const double k = r_int * r_int * r_int * (dtf_int - out_int);
+  const double rinv = 1.0 / r;
+  rhs[idx] = -c * (dfdr + (fv - finf) * rinv) + k * rinv * rinv * rinv;
+}
+
+int launch_radiation_batched(int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts, cudaStream_t s) {
+  if (npts <= 0) return BSSN_B200_OK;
+  const int threads = 256;
+  const long long work = (long long)npts * NUM_EVOL_GFS;
+  radiation_batched_kernel<<<(unsigned)((work + threads - 1) / threads), threads, 0, s>>>(descs, pts, npts, stage);
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+// Parity copies into every inner ghost point of every evolution's stage output.
+__global__ void inner_batched_kernel(const EvoDesc *__restrict__ descs, const BatchInnerPt *__restrict__ pts,
+                                     const int npts, const int stage) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * NUM_EVOL_GFS) return;
+  const int gf = t / npts;
+  const BatchInnerPt q = pts[t - gf * npts];
+  const EvoDesc &d = descs[q.evo];
+  double *kin, *kout;
+  stage_io(d, stage, kin, kout);
+  double *g = kout + (size_t)gf * d.g.ntot;
+  constexpr int8_t parity[NUM_EVOL_GFS] = {4, 5, 6, 7, 8, 9, 0, 1, 2, 3, 0, 4, 5, 6, 7, 8, 9, 1, 2, 3, 0, 1, 2, 3};
+  g[q.b.dstpt] = flip_sign(g[q.b.srcpt], q.b.parity[parity[gf]]);
+}
+
+int launch_inner_batched(int stage, const EvoDesc *descs, const BatchInnerPt *pts, int npts, cudaStream_t s) {
+  if (npts <= 0) return BSSN_B200_OK;
+  const int threads = 256;
+  const long long work = (long long)npts * NUM_EVOL_GFS;
+  inner_batched_kernel<<<(unsigned)((work + threads - 1) / threads), threads, 0, s>>>(descs, pts, npts, stage);
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
 }  // namespace bssn

@@ -122,6 +122,49 @@ int launch_radiation_rk_bcs(Variant v, const GridDims &g, const params_struct *p
                             const double *const xx[3], const RfmArrays &rfm, int stage, double dt,
                             const StageBuffers &b, double *krhs_scratch, cudaStream_t s);
 
+// ---------------------------------------------------------------- batched evolutions
+// One independent evolution of a batch, as the device sees it. Stage buffers rotate as in
+// a single-grid RK4 step: stage 1 reads y and writes k_odd, 2: k_odd -> k_even,
+// 3: k_even -> k_odd, 4: k_odd -> y.
+struct EvoDesc {
+  GridDims g;
+  RfmArrays rfm;
+  PhysParams pp;
+  double dt;
+  double *y, *run, *kodd, *keven, *aux, *krhs;
+  const double *xx0;
+  int radial_sinh;  // 0: r = xx0 ; 1: SinhSpherical r(xx0)
+  double AMPL, SINHW;
+  int tile_begin, tiles_x, tiles_y;  // this evolution's tiles in the batch tile list
+};
+struct BatchOuterPt {
+  int evo;
+  outerpt_bc_struct p;
+};
+struct BatchInnerPt {
+  int evo;
+  innerpt_bc_struct b;
+};
+__host__ __device__ inline void stage_io(const EvoDesc &d, int stage, double *&kin, double *&kout) {
+  switch (stage) {
+    case 1: kin = d.y; kout = d.kodd; break;
+    case 2: kin = d.kodd; kout = d.keven; break;
+    case 3: kin = d.keven; kout = d.kodd; break;
+    default: kin = d.kodd; kout = d.y; break;
+  }
+}
+// Batched launchers (pointwise.cu, boundary.cu): one launch covers every evolution.
+// `blocks` is the persistent grid size; the block shape (bx, by) with bx*by = 128 is the
+// tile shape the tile list was built for.
+int launch_ricci_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
+                         int bx, int by, cudaStream_t s);
+int launch_rhs_fused_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
+                             int bx, int by, cudaStream_t s);
+int launch_radiation_batched(int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts, cudaStream_t s);
+int launch_rk_points_batched(Variant v, int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts,
+                             cudaStream_t s);
+int launch_inner_batched(int stage, const EvoDesc *descs, const BatchInnerPt *pts, int npts, cudaStream_t s);
+
 // Device constants (wave speeds, asymptotic values, parity types).
 extern const int8_t kEvolParity[NUM_EVOL_GFS];
 extern const double kWavespeed[NUM_EVOL_GFS];

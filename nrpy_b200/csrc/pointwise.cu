@@ -127,21 +127,27 @@ static dim3 interior_grid(const GridDims &g) {
 template <typename T>
 __device__ __forceinline__ volatile T *thread_slots() {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + BX * threadIdx.y);
+  return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + blockDim.x * threadIdx.y);
 }
 
 template <Variant V, int G>
-__global__ void __launch_bounds__(BX *BY, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
-                                                          const double *__restrict__ in, double *__restrict__ aux) {
+__device__ __forceinline__ void ricci_body(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux,
+                                           int i0, int i1, int i2, volatile double *sm) {
   using Grp = RicciG<V, G>;
-  volatile double *sm = thread_slots<double>();
-  INTERIOR_INDEX_OR_RETURN(g);
   const PointCtx ctx = make_ctx(g, rfm, in, nullptr, i0, i1, i2);
   double out[Grp::N];
   Grp::template eval<double, double>(ctx, out, sm);
   const int idx = i0 + g.s1 * i1 + g.s2 * i2;
 #pragma unroll
   for (int k = 0; k < Grp::N; k++) aux[idx + Grp::GF(k) * g.ntot] = out[k];
+}
+
+template <Variant V, int G>
+__global__ void __launch_bounds__(BX *BY, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
+                                                          const double *__restrict__ in, double *__restrict__ aux) {
+  volatile double *sm = thread_slots<double>();
+  INTERIOR_INDEX_OR_RETURN(g);
+  ricci_body<V, G>(g, rfm, in, aux, i0, i1, i2, sm);
 }
 
 template <Variant V, typename T, int G>
@@ -250,12 +256,10 @@ __device__ __forceinline__ void rk_and_project_point(const GridDims &g, const Rf
 // projection to the new hDD. The raw RHS is also stored to `krhs` on the interior shell
 // (the layer next to each face), where the outer radiation condition reads it.
 template <Variant V, typename T, int STAGE, int G>
-__global__ void __launch_bounds__(BX *BY, 1) rhs_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
-                                                              const double *__restrict__ aux, const StageBuffers b,
-                                                              double *__restrict__ krhs, const double dt) {
+__device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
+                                           const double *aux, const StageBuffers &b, double *krhs, const double dt,
+                                           int i0, int i1, int i2, volatile T *sm) {
   using Grp = RhsG<V, G>;
-  volatile T *sm = thread_slots<T>();
-  INTERIOR_INDEX_OR_RETURN(g);
   PointCtx ctx = make_ctx(g, rfm, b.kin, aux, i0, i1, i2);
   ctx.eta = pp.eta;
   ctx.KreissOliger_strength_gauge = pp.ko_gauge;
@@ -289,6 +293,19 @@ __global__ void __launch_bounds__(BX *BY, 1) rhs_fused_kernel(const GridDims g, 
   }
 #pragma unroll
   for (int k = 0; k < Grp::N; k++) b.kout[idx + (size_t)Grp::GF(k) * g.ntot] = o[Grp::GF(k)];
+}
+
+// One output group of the RHS at an interior point, then in registers the RK4 stage update
+// of that group's gridfunctions; the group holding hDD also applies the detgammabar
+// projection to the new hDD. The raw RHS is also stored to `krhs` on the interior shell
+// (the layer next to each face), where the outer radiation condition reads it.
+template <Variant V, typename T, int STAGE, int G>
+__global__ void __launch_bounds__(BX *BY, 1) rhs_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
+                                                              const double *__restrict__ aux, const StageBuffers b,
+                                                              double *__restrict__ krhs, const double dt) {
+  volatile T *sm = thread_slots<T>();
+  INTERIOR_INDEX_OR_RETURN(g);
+  fused_body<V, T, STAGE, G>(g, rfm, pp, aux, b, krhs, dt, i0, i1, i2, sm);
 }
 
 // RK update plus projection of listed boundary points whose RHS is already in krhs.
@@ -474,6 +491,173 @@ int launch_rk_points(Variant v, int stage, double dt, const GridDims &g, const R
                      const outerpt_bc_struct *pts, int npts, const double *krhs, cudaStream_t s) {
   if (npts <= 0) return BSSN_B200_OK;
   VARIANT_SWITCH(v, (launch_rk_points_typed<VV>(stage, g, rfm, b, pts, npts, krhs, dt, s)));
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+// ---------------------------------------------------------------- batched evolutions
+// Persistent kernels over a tile list that spans every evolution of a batch: block b takes
+// tiles b, b + gridDim.x, ... Tile t belongs to evolution tile_evo[t]; its local index runs
+// over (tiles_x, tiles_y, n2) tiles of blockDim.x x blockDim.y interior points.
+__device__ __forceinline__ bool tile_point(const EvoDesc &d, int t_local, int &i0, int &i1, int &i2) {
+  const int tx = t_local % d.tiles_x;
+  const int r = t_local / d.tiles_x;
+  const int ty = r % d.tiles_y;
+  const int tz = r / d.tiles_y;
+  i0 = NGHOSTS + tx * blockDim.x + threadIdx.x;
+  i1 = NGHOSTS + ty * blockDim.y + threadIdx.y;
+  i2 = NGHOSTS + tz;
+  return i0 < d.g.N0 - NGHOSTS && i1 < d.g.N1 - NGHOSTS;
+}
+
+template <Variant V, int G>
+__global__ void __launch_bounds__(BX *BY, 1) ricci_batched_kernel(const EvoDesc *__restrict__ descs,
+                                                                  const int *__restrict__ tile_evo, const int ntiles,
+                                                                  const int stage) {
+  volatile double *sm = thread_slots<double>();
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const EvoDesc &d = descs[tile_evo[t]];
+    int i0, i1, i2;
+    if (!tile_point(d, t - d.tile_begin, i0, i1, i2)) continue;
+    double *kin, *kout;
+    stage_io(d, stage, kin, kout);
+    ricci_body<V, G>(d.g, d.rfm, kin, d.aux, i0, i1, i2, sm);
+  }
+}
+
+template <Variant V, int STAGE, int G>
+__global__ void __launch_bounds__(BX *BY, 1) rhs_fused_batched_kernel(const EvoDesc *__restrict__ descs,
+                                                                      const int *__restrict__ tile_evo,
+                                                                      const int ntiles) {
+  volatile double *sm = thread_slots<double>();
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const EvoDesc &d = descs[tile_evo[t]];
+    int i0, i1, i2;
+    if (!tile_point(d, t - d.tile_begin, i0, i1, i2)) continue;
+    StageBuffers b;
+    b.y = d.y;
+    b.run = d.run;
+    stage_io(d, STAGE, b.kin, b.kout);
+    fused_body<V, double, STAGE, G>(d.g, d.rfm, d.pp, d.aux, b, d.krhs, d.dt, i0, i1, i2, sm);
+  }
+}
+
+template <Variant V, int STAGE>
+__global__ void rk_points_batched_kernel(const EvoDesc *__restrict__ descs, const BatchOuterPt *__restrict__ pts,
+                                         const int npts) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts) return;
+  const BatchOuterPt q = pts[t];
+  const EvoDesc &d = descs[q.evo];
+  StageBuffers b;
+  b.y = d.y;
+  b.run = d.run;
+  stage_io(d, STAGE, b.kin, b.kout);
+  const int idx = q.p.i0 + d.g.s1 * q.p.i1 + d.g.s2 * q.p.i2;
+  double kk[NUM_EVOL_GFS];
+#pragma unroll
+  for (int k = 0; k < NUM_EVOL_GFS; k++) kk[k] = d.krhs[idx + (size_t)k * d.g.ntot];
+  rk_and_project_point<V, STAGE>(d.g, d.rfm, b, idx, q.p.i0, q.p.i1, kk, d.dt);
+}
+
+template <Variant V, int G>
+static int launch_ricci_batched_group(int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
+                                      int bx, int by, cudaStream_t s) {
+  using Grp = RicciG<V, G>;
+  constexpr size_t sb = slot_bytes<Grp, double>();
+  BSSN_TRY(set_smem(ricci_batched_kernel<V, G>, sb));
+  ricci_batched_kernel<V, G><<<blocks, dim3(bx, by), sb, s>>>(descs, tile_evo, ntiles, stage);
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+template <Variant V, int STAGE, int G>
+static int launch_fused_batched_group(const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks, int bx,
+                                      int by, cudaStream_t s) {
+  using Grp = RhsG<V, G>;
+  constexpr size_t sb = slot_bytes<Grp, double>();
+  BSSN_TRY(set_smem(rhs_fused_batched_kernel<V, STAGE, G>, sb));
+  rhs_fused_batched_kernel<V, STAGE, G><<<blocks, dim3(bx, by), sb, s>>>(descs, tile_evo, ntiles);
+  BSSN_LAUNCH_CHECK();
+  return BSSN_B200_OK;
+}
+
+template <Variant V, int STAGE>
+static int launch_fused_batched_stage(const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks, int bx,
+                                      int by, cudaStream_t s) {
+  BSSN_TRY((launch_fused_batched_group<V, STAGE, 0>(descs, tile_evo, ntiles, blocks, bx, by, s)));
+  BSSN_TRY((launch_fused_batched_group<V, STAGE, 1>(descs, tile_evo, ntiles, blocks, bx, by, s)));
+  return launch_fused_batched_group<V, STAGE, 2>(descs, tile_evo, ntiles, blocks, bx, by, s);
+}
+
+static int check_shape(int bx, int by) {
+  if (bx * by != BX * BY || bx < 1 || by < 1) {
+    set_error("batched tile shape %dx%d: must have %d threads", bx, by, BX * BY);
+    return BSSN_B200_EINVAL;
+  }
+  return BSSN_B200_OK;
+}
+
+int launch_ricci_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
+                         int bx, int by, cudaStream_t s) {
+  BSSN_TRY(check_shape(bx, by));
+  if (ntiles <= 0) return BSSN_B200_OK;
+  if (v != SPH_3D && v != SINH_3D) {
+    set_error("batched evolutions: only full 3-D variants are instantiated");
+    return BSSN_B200_EINVAL;
+  }
+  if (v == SPH_3D) {
+    BSSN_TRY((launch_ricci_batched_group<SPH_3D, 0>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
+    BSSN_TRY((launch_ricci_batched_group<SPH_3D, 1>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
+    return launch_ricci_batched_group<SPH_3D, 2>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+  }
+  BSSN_TRY((launch_ricci_batched_group<SINH_3D, 0>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
+  BSSN_TRY((launch_ricci_batched_group<SINH_3D, 1>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
+  return launch_ricci_batched_group<SINH_3D, 2>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+}
+
+template <Variant V>
+static int launch_fused_batched_v(int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
+                                  int bx, int by, cudaStream_t s) {
+  switch (stage) {
+    case 1: return launch_fused_batched_stage<V, 1>(descs, tile_evo, ntiles, blocks, bx, by, s);
+    case 2: return launch_fused_batched_stage<V, 2>(descs, tile_evo, ntiles, blocks, bx, by, s);
+    case 3: return launch_fused_batched_stage<V, 3>(descs, tile_evo, ntiles, blocks, bx, by, s);
+    default: return launch_fused_batched_stage<V, 4>(descs, tile_evo, ntiles, blocks, bx, by, s);
+  }
+}
+
+int launch_rhs_fused_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
+                             int bx, int by, cudaStream_t s) {
+  BSSN_TRY(check_shape(bx, by));
+  if (ntiles <= 0) return BSSN_B200_OK;
+  if (v == SPH_3D) return launch_fused_batched_v<SPH_3D>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+  if (v == SINH_3D) return launch_fused_batched_v<SINH_3D>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+  set_error("batched evolutions: only full 3-D variants are instantiated");
+  return BSSN_B200_EINVAL;
+}
+
+template <Variant V>
+static void launch_rk_points_batched_v(int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts,
+                                       cudaStream_t s) {
+  const int threads = 128, blocks = (npts + threads - 1) / threads;
+  switch (stage) {
+    case 1: rk_points_batched_kernel<V, 1><<<blocks, threads, 0, s>>>(descs, pts, npts); break;
+    case 2: rk_points_batched_kernel<V, 2><<<blocks, threads, 0, s>>>(descs, pts, npts); break;
+    case 3: rk_points_batched_kernel<V, 3><<<blocks, threads, 0, s>>>(descs, pts, npts); break;
+    default: rk_points_batched_kernel<V, 4><<<blocks, threads, 0, s>>>(descs, pts, npts); break;
+  }
+}
+
+int launch_rk_points_batched(Variant v, int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts,
+                             cudaStream_t s) {
+  if (npts <= 0) return BSSN_B200_OK;
+  if (v == SPH_3D) launch_rk_points_batched_v<SPH_3D>(stage, descs, pts, npts, s);
+  else if (v == SINH_3D) launch_rk_points_batched_v<SINH_3D>(stage, descs, pts, npts, s);
+  else {
+    set_error("batched evolutions: only full 3-D variants are instantiated");
+    return BSSN_B200_EINVAL;
+  }
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
