@@ -178,6 +178,9 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--nxx", default=None, help="override the grid, e.g. 256,64,32 (profiling only)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -243,6 +246,9 @@ def main():
     value, ms = aggregate(pts, args.steps, ms, dist, device="cuda")
     clocks = clk.summary()
 
+    y_fp64 = grid.y_n.clone()
+    mixed = None if args.no_mixed else run_mixed(grid, args, y0, y_fp64, h_hist, stream)
+
     # ---------------- dominant kernel alone: fused interior RHS + RK update, per stage
     kstats = time_fused_kernel(grid, lib, stream, reps=5)
     peak, peak_kind = peaks()
@@ -251,7 +257,12 @@ def main():
 
     # ---------------- end-to-end through the public API with host buffers
     e2e = None if args.no_e2e else run_e2e(grid, args, y0)
+    grid_dt = grid.dt
     grid.free_stepper()
+    grid.close()
+    del grid, y0, y_fp64
+    torch.cuda.empty_cache()
+    batched = None if args.no_batched else run_batched(args, world, rank, dist)
 
     if rank == 0:
         cpu = None
@@ -269,8 +280,8 @@ def main():
                        "interior_points": pts, "mode": "fused stages" if args.mode == 1 else "reference stage order",
                        "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",
                        "parallelism": f"replicas x{world}", "seed": args.seed, "bl": [m1, z1, m2, z2],
-                       "dt": grid.dt, "H_L2_last": h_hist[-1] if h_hist else None},
-            "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel (interior RHS + RK4 update + projection)",
+                       "dt": grid_dt, "H_L2_last": h_hist[-1] if h_hist else None},
+            "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel, groups 0-2 (one interior RK stage: RHS + RK4 update + projection)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": None,
                          "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": kstats["ms_per_launch"],
@@ -280,12 +291,108 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "mixed": mixed,
+            "batched": batched,
         }
         print(json.dumps(line))
-    grid.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_mixed(grid, args, y0, y_fp64, h_fp64, stream):
+    """Same workload with the Ricci/RHS algebra in FP32 (stencils, state, RK accumulation,
+    detgammabar projection and constraint reductions in FP64): rate, H-constraint L2 next
+    to the FP64 run's, and the per-gridfunction relative L2 of the final state vs FP64."""
+    import torch
+
+    grid.free_stepper()
+    grid.y_n.copy_(y0)
+    st = grid.make_stepper(mode=args.mode, mixed=True, steps_per_graph=1)
+    with torch.cuda.stream(st):
+        grid.run_stepper(args.warmup)
+    torch.cuda.synchronize()
+    grid.y_n.copy_(y0)
+    torch.cuda.synchronize()
+    h = []
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        a.record(st)
+        done = 0
+        while done < args.steps:
+            n = min(H_EVERY, args.steps - done)
+            grid.run_stepper(n)
+            done += n
+            if done % H_EVERY == 0:
+                h.append(grid.constraint_norms()["H_L2"])
+        b.record(st)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    m = grid.y_n.view(24, -1)
+    f = y_fp64.view(24, -1)
+    num = torch.linalg.vector_norm(m - f, dim=1)
+    den = torch.linalg.vector_norm(f, dim=1).clamp_min(1e-300)
+    rel = (num / den).cpu().numpy()
+    nz = (torch.linalg.vector_norm(f, dim=1) > 1e-12 * torch.linalg.vector_norm(f, dim=1).max()).cpu().numpy()
+    grid.free_stepper()
+    return {"value": grid.n_interior * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "dtype": "f32 algebra / f64 state", "H_L2": h[-1] if h else None,
+            "H_L2_fp64": h_fp64[-1] if h_fp64 else None,
+            "H_L2_rel_diff": (abs(h[-1] - h_fp64[-1]) / h_fp64[-1]) if h and h_fp64 else None,
+            "rel_l2_vs_fp64_max": float(rel[nz].max()) if nz.any() else None,
+            "rel_l2_vs_fp64_per_gf": [float(x) for x in rel]}
+
+
+def run_batched(args, world, rank, dist):
+    """64 independent Brill-Lindquist evolutions (Spherical, Nxx ~ [48..128]x[8..32]x[2..16])
+    advanced together: autotuned tile shape, one captured CUDA graph of 20 RK4 steps
+    replayed; compared with the same evolutions advanced one grid at a time."""
+    import torch
+
+    from nrpy_b200.batch import BatchedEvolutions, batching_workload, partition_evolutions
+
+    specs = batching_workload(seed=7, n=64)
+    sizes = [s["Nxx"][0] * s["Nxx"][1] * s["Nxx"][2] for s in specs]
+    mine = partition_evolutions(sizes, world)[rank]
+    be = BatchedEvolutions([specs[i] for i in mine])
+    tune = be.autotune(steps=2)
+    spg = 20
+    be.build(tile=tune["tile"], blocks=tune["blocks"], steps_per_graph=spg)
+    be.run(1)
+    torch.cuda.synchronize()
+    steps = max(spg, (args.batch_steps // spg) * spg)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(be.stream)
+    be.run(steps // spg)
+    b.record(be.stream)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    pts = be.interior_points
+    value, ms_max = aggregate(pts, steps, ms, dist, device="cuda")
+    info = be.info()
+    be.free()
+    # the same evolutions one grid at a time (single-grid CUDA graphs), a few steps each
+    seq_steps = 10
+    seq_ms = 0.0
+    for g in be.grids:
+        st = g.make_stepper(mode=1, steps_per_graph=seq_steps)
+        with torch.cuda.stream(st):
+            g.run_stepper(1)
+        torch.cuda.synchronize()
+        a2, b2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a2.record(st)
+        with torch.cuda.stream(st):
+            g.run_stepper(1)
+        b2.record(st)
+        b2.synchronize()
+        seq_ms += a2.elapsed_time(b2)
+        g.free_stepper()
+    seq_value, _ = aggregate(pts, seq_steps, seq_ms, dist, device="cuda")
+    be.close()
+    return {"value": value, "unit": UNIT, "evolutions": len(specs), "steps": steps, "ms_per_step": ms_max / steps,
+            "interior_points": pts if dist is None else None, "tile": list(tune["tile"]), "blocks": tune["blocks"],
+            "autotune": tune["table"], "graph_kernel_nodes_per_replay": info["kernel_nodes"],
+            "sequential_single_grid_value": seq_value, "speedup_vs_sequential": value / seq_value}
 
 
 def time_fused_kernel(grid, lib, stream, reps: int = 5):

@@ -24,11 +24,15 @@ TILE_SHAPES = [(32, 4), (64, 2), (16, 8), (128, 1)]
 
 def batching_workload(seed: int = 7, n: int = 64) -> List[Dict]:
     """The batched workload: n evolutions on Spherical grids with Nxx drawn from
-    [48..128] x [8..32] x [2..16], masses ~U[0.3,0.7], separations ~U[0.6,1.6] (z = +/-sep/2)."""
+    [48..128] x [8..32] x [2..16], masses ~U[0.3,0.7], separations ~U[0.6,1.6] (z = +/-sep/2).
+
+    Nxx2 is drawn among the even values: on a cell-centred phi grid the inner-boundary map
+    across the polar axis sends phi to phi + pi, which is a grid point only when Nxx2 is even
+    (bcstruct_set_up rejects odd Nxx2 for full 3-D Spherical grids)."""
     rng = np.random.default_rng(seed)
     specs = []
     for _ in range(n):
-        nxx = (int(rng.integers(48, 129)), int(rng.integers(8, 33)), int(rng.integers(2, 17)))
+        nxx = (int(rng.integers(48, 129)), int(rng.integers(8, 33)), 2 * int(rng.integers(1, 9)))
         m1, m2 = rng.uniform(0.3, 0.7, 2)
         sep = rng.uniform(0.6, 1.6)
         specs.append(dict(coord="Spherical", Nxx=nxx, grid_physical_size=7.5, BH1_mass=float(m1),

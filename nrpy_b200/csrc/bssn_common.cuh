@@ -82,7 +82,9 @@ struct PhysParams {
 };
 
 // Pointwise operators implemented in pointwise.cu.
-int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s);
+// mixed = true evaluates the algebra in FP32 (stencils, inputs and outputs stay FP64).
+int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s,
+                 bool mixed = false);
 int launch_rhs(Variant v, bool mixed, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
                const double *aux, const double *in, double *rhs, cudaStream_t s);
 int launch_constraints(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, const double *aux,

@@ -130,24 +130,24 @@ __device__ __forceinline__ volatile T *thread_slots() {
   return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + blockDim.x * threadIdx.y);
 }
 
-template <Variant V, int G>
+template <Variant V, int G, typename T = double>
 __device__ __forceinline__ void ricci_body(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux,
-                                           int i0, int i1, int i2, volatile double *sm) {
+                                           int i0, int i1, int i2, volatile T *sm) {
   using Grp = RicciG<V, G>;
   const PointCtx ctx = make_ctx(g, rfm, in, nullptr, i0, i1, i2);
-  double out[Grp::N];
-  Grp::template eval<double, double>(ctx, out, sm);
+  T out[Grp::N];
+  Grp::template eval<T, double>(ctx, out, sm);
   const int idx = i0 + g.s1 * i1 + g.s2 * i2;
 #pragma unroll
-  for (int k = 0; k < Grp::N; k++) aux[idx + Grp::GF(k) * g.ntot] = out[k];
+  for (int k = 0; k < Grp::N; k++) aux[idx + Grp::GF(k) * g.ntot] = double(out[k]);
 }
 
-template <Variant V, int G>
+template <Variant V, int G, typename T>
 __global__ void __launch_bounds__(BX *BY, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
                                                           const double *__restrict__ in, double *__restrict__ aux) {
-  volatile double *sm = thread_slots<double>();
+  volatile T *sm = thread_slots<T>();
   INTERIOR_INDEX_OR_RETURN(g);
-  ricci_body<V, G>(g, rfm, in, aux, i0, i1, i2, sm);
+  ricci_body<V, G, T>(g, rfm, in, aux, i0, i1, i2, sm);
 }
 
 template <Variant V, typename T, int G>
@@ -349,27 +349,32 @@ static int set_smem(KernelPtr k, size_t bytes) {
   return BSSN_B200_OK;
 }
 
-template <Variant V, int G>
+template <Variant V, int G, typename T>
 static int launch_ricci_group(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
   using Grp = RicciG<V, G>;
-  constexpr size_t sb = slot_bytes<Grp, double>();
-  BSSN_TRY(set_smem(ricci_kernel<V, G>, sb));
-  ricci_kernel<V, G><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, in, aux);
+  constexpr size_t sb = slot_bytes<Grp, T>();
+  BSSN_TRY(set_smem(ricci_kernel<V, G, T>, sb));
+  ricci_kernel<V, G, T><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, in, aux);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
 
-template <Variant V>
+template <Variant V, typename T>
 static int launch_ricci_v(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
   static_assert(kRicciGroups == 3, "group count");
-  BSSN_TRY((launch_ricci_group<V, 0>(g, rfm, in, aux, s)));
-  BSSN_TRY((launch_ricci_group<V, 1>(g, rfm, in, aux, s)));
-  return launch_ricci_group<V, 2>(g, rfm, in, aux, s);
+  BSSN_TRY((launch_ricci_group<V, 0, T>(g, rfm, in, aux, s)));
+  BSSN_TRY((launch_ricci_group<V, 1, T>(g, rfm, in, aux, s)));
+  return launch_ricci_group<V, 2, T>(g, rfm, in, aux, s);
 }
 
-int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
+int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s,
+                 bool mixed) {
   if (empty_interior(g)) return BSSN_B200_OK;
-  VARIANT_SWITCH(v, return launch_ricci_v<VV>(g, rfm, in, aux, s));
+  if (mixed) {
+    VARIANT_SWITCH(v, return (launch_ricci_v<VV, float>(g, rfm, in, aux, s)));
+  } else {
+    VARIANT_SWITCH(v, return (launch_ricci_v<VV, double>(g, rfm, in, aux, s)));
+  }
   return BSSN_B200_OK;
 }
 
@@ -521,7 +526,7 @@ __global__ void __launch_bounds__(BX *BY, 1) ricci_batched_kernel(const EvoDesc 
     if (!tile_point(d, t - d.tile_begin, i0, i1, i2)) continue;
     double *kin, *kout;
     stage_io(d, stage, kin, kout);
-    ricci_body<V, G>(d.g, d.rfm, kin, d.aux, i0, i1, i2, sm);
+    ricci_body<V, G, double>(d.g, d.rfm, kin, d.aux, i0, i1, i2, sm);
   }
 }
 
