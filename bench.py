@@ -59,6 +59,18 @@ def aggregate(pts_local: int, steps: int, ms_local: float, dist=None, device="cp
     return float(n.item()) / (float(t.item()) * 1e-3), float(t.item())
 
 
+def profiled_traffic():
+    """DRAM bytes per fused stage pass at the bench size, from the committed ncu summary."""
+    p = ROOT / "profiles" / "kernels_rhs_ricci_groups_sinh256x64x32.md"
+    try:
+        for line in p.read_text().splitlines():
+            if line.startswith("traffic_bytes_per_launch_full_size:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -283,7 +295,10 @@ def main():
                        "dt": grid_dt, "H_L2_last": h_hist[-1] if h_hist else None},
             "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel, groups 0-2 (one interior RK stage: RHS + RK4 update + projection)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind, "traffic": None,
+                         "peak_source": peak_kind,
+                         "traffic": profiled_traffic() if NXX == (256, 64, 64) else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the three group "
+                                           "launches of one stage at 256x64x32, scaled by point count",
                          "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": kstats["ms_per_launch"],
                          "step_achieved": value / world * B_ALG_PER_PT_STEP / 1e9,
                          "step_frac": value / world * B_ALG_PER_PT_STEP / 1e9 / peak},
