@@ -109,7 +109,7 @@ static int host_xx(const params_struct *p, REAL *const xx[3], std::vector<double
 int grid_params(const commondata_struct *cd, params_struct *p, REAL *xx[3], const int Nx[3], bool apply_defaults) {
   Coord c;
   BSSN_TRY(coord_of(p, &c));
-  if (Nx[0] != -1 && Nx[1] != -1 && Nx[2] != -1) {
+  if (Nx != nullptr && Nx[0] != -1 && Nx[1] != -1 && Nx[2] != -1) {
     p->Nxx0 = Nx[0];
     p->Nxx1 = Nx[1];
     p->Nxx2 = Nx[2];
