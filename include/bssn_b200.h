@@ -330,6 +330,32 @@ int bssn_b200_batch_info(const bssn_b200_batch *batch, int *ntiles, int *nouter,
                          unsigned long long *kernel_nodes);
 int bssn_b200_batch_destroy(bssn_b200_batch *batch);
 
+/* Reverse mode (no counterpart in the reference, which has no adjoint). Gradient of
+ *   J = sum over interior points of H^2 + alpha(NGHOSTS, N1/2, N2/2)
+ * after `nsteps` RK4 steps (radiation outer BCs) with respect to the Brill-Lindquist
+ * parameters (BH1_mass, BH1_posn_z, BH2_mass, BH2_posn_z) of the initial data, by the
+ * discrete adjoint of the stage-by-stage step (mode 0 of bssn_b200_mol_step). The forward
+ * keeps y every `checkpoint_every` steps; the backward recomputes each segment from its
+ * checkpoint. Spherical coordinates without symmetry axes; one grid (NUMGRIDS = 1).
+ * The handle uses the grid's MoL storage as workspace: after backward, y_n_gfs holds the
+ * final state again. `stream` as in the other entry points. */
+typedef struct bssn_b200_adjoint bssn_b200_adjoint;
+int bssn_b200_adjoint_create(commondata_struct *commondata, griddata_struct *griddata, int nsteps,
+                             int checkpoint_every, void *stream, bssn_b200_adjoint **out);
+/* Evolve y_n_gfs (the initial data) nsteps steps; out = {J, sum H^2, alpha term} (host). */
+int bssn_b200_adjoint_forward(bssn_b200_adjoint *adj, double out[3]);
+/* grad (host, 4) = Jbar * dJ/d(BH1_mass, BH1_posn_z, BH2_mass, BH2_posn_z); optionally the
+ * adjoint of the initial state y_0 into ybar0 (device, NUM_EVOL_GFS gridfunctions). */
+int bssn_b200_adjoint_backward(bssn_b200_adjoint *adj, double Jbar, double *ybar0, double grad[4]);
+/* Pieces of the chain on a given device state y (NUM_EVOL_GFS gridfunctions):
+ * J(y); ybar = Jbar dJ/dy; ybar <- (dF/dy)^T ybar for one RK4 step F at y_n;
+ * grad from the adjoint of y_0 through the initial-data BCs and psi^-2. */
+int bssn_b200_adjoint_functional(bssn_b200_adjoint *adj, const double *y, double out[3]);
+int bssn_b200_adjoint_functional_vjp(bssn_b200_adjoint *adj, const double *y, double Jbar, double *ybar);
+int bssn_b200_adjoint_step_vjp(bssn_b200_adjoint *adj, const double *y_n, double *ybar);
+int bssn_b200_adjoint_id_vjp(bssn_b200_adjoint *adj, const double *ybar0, double grad[4]);
+int bssn_b200_adjoint_destroy(bssn_b200_adjoint *adj);
+
 /* Instrumentation: kernels launched by this library since it was loaded (each graph replay
  * counts its kernel nodes), and a launch of only the interior RHS + RK-update + projection
  * kernel of RK4 stage `stage` (1..4) of grid 0, used to time the dominant kernel alone.

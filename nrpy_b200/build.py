@@ -19,7 +19,8 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libbssn_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["abi.cu", "setup.cu", "pointwise.cu", "boundary.cu", "mol.cu", "reductions.cu", "batch.cu"]
+SOURCES = ["abi.cu", "setup.cu", "pointwise.cu", "boundary.cu", "mol.cu", "reductions.cu", "batch.cu",
+           "adjoint.cu"]
 
 
 def nvcc() -> str:
@@ -41,7 +42,9 @@ def _newest_dep(src: str) -> float:
     """Newest modification time among a source and the headers it can include."""
     deps = [CSRC / src, CSRC / "bssn_common.cuh"] + list((ROOT / "include").glob("*.h"))
     if src == "pointwise.cu":
-        deps += list((CSRC / "gen").glob("*.cuh"))
+        deps += [p for p in (CSRC / "gen").glob("bssn_*.cuh") if not p.name.startswith("bssn_adj_")]
+    if src == "adjoint.cu":
+        deps += list((CSRC / "gen").glob("bssn_adj_*.cuh"))
     return max(p.stat().st_mtime for p in deps)
 
 

@@ -108,12 +108,19 @@ class _Printer(C99CodePrinter):
             return f"(T(1.0)/cbrt({self._print(b)}))"
         if e == sp.Rational(2, 3):
             return f"(cbrt({self._print(b)})*cbrt({self._print(b)}))"
+        if e.is_Rational and int(e.q) in (2, 3):
+            root = f"{'sqrt' if int(e.q) == 2 else 'cbrt'}({self._print(b)})"
+            mag = abs(int(e.p))
+            prod = "*".join([root] * mag) if mag <= 4 else f"ipow({root}, {mag})"
+            return f"({prod})" if e > 0 else f"(T(1.0)/({prod}))"
         raise NotImplementedError(f"power {expr}")
 
     def _print_Function(self, expr):
         fname = expr.func.__name__
-        if fname == "nrpyAbs":
+        if fname in ("nrpyAbs", "_Abs"):
             return f"fabs({self._print(expr.args[0])})"
+        if fname == "_Sign":
+            return f"copysign(T(1.0), {self._print(expr.args[0])})"
         return super()._print_Function(expr)
 
     def _print_Abs(self, expr):
@@ -166,6 +173,10 @@ class PointKernel:
             return
         if name in SCALAR_PARAMS:
             self.lines.append(f"const T {name} = T(PARAM({name}));")
+            return
+        m = re.fullmatch(r"AO(\d+)", name)
+        if m:  # adjoint seed of forward output m (reverse-mode functions)
+            self.lines.append(f"const T {name} = T(ADJIN({m.group(1)}));")
             return
         pd = parse_deriv(name)
         if pd is None:
@@ -284,6 +295,29 @@ class PointKernel:
                               else f"const T {name} = {self.printer._print(e)};")
         self.lines = schedule_lines(self.lines)
         return "\n".join("  " + ln for ln in self.lines)
+
+    def build_program(self, stmts: Sequence[Tuple[str, sp.Expr]], outputs: Sequence[Tuple[str, sp.Expr]],
+                      upwind_vec=None) -> None:
+        """Emit an already-CSE'd straight-line program (name, expr) and then the outputs
+        (lhs code, expr); long sums are split into partial-sum chains as in build()."""
+        self.upwind_vec = upwind_vec
+        pos = {name: i for i, (name, _) in enumerate(stmts)}
+
+        def order_of(x):
+            return pos.get(x.name, -1)
+
+        flat: List[Tuple[str, sp.Expr, bool]] = []
+        for name, e in stmts:
+            flat += [(n, x, False) for n, x in self._chain(name, e, order_of)]
+        for k, (lhs, e) in enumerate(outputs):
+            chain = self._chain(f"_res{k}", e, order_of)
+            flat += [(n, x, False) for n, x in chain[:-1]]
+            flat.append((lhs, chain[-1][1], True))
+        for name, e, is_out in flat:
+            self._ensure(e)
+            self.lines.append(f"{name} = {self.printer._print(e)};" if is_out
+                              else f"const T {name} = {self.printer._print(e)};")
+        self.lines = schedule_lines(self.lines)
 
 
 _DEF_RE = re.compile(r"\s*const (?:T|double|bool) (\w+) =")

@@ -36,6 +36,10 @@ RHS_GROUPS = [
     ["betU0", "betU1", "betU2", "lambdaU0", "lambdaU1", "lambdaU2"],
 ]
 REG_CAPACITY = 90
+# Reverse-mode (adjoint) functions: generated for these variants only; fewer values in
+# registers because the VJP kernels run 64 threads per block with shared-memory slots.
+ADJOINT_VARIANTS = ["sph_3d"]
+ADJ_REG_CAPACITY = 64
 
 
 def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int) -> str:
@@ -126,21 +130,155 @@ def generate_variant(tag: str) -> None:
     print(f"{tag}: {stats} ({time.time() - t0:.1f}s)")
 
 
+def _c_rational(r) -> str:
+    import sympy as sp
+
+    r = sp.Rational(r)
+    return f"{int(r.p)}.0" if r.q == 1 else f"{int(r.p)}.0 / {int(r.q)}.0"
+
+
+def _vjp_struct(kind: str, tag: str, g: int, fname: str, seeds, slots: int) -> str:
+    cases = " ".join(f"case {k}: return {x};" for k, x in enumerate(seeds))
+    return (
+        f"template <> struct {kind}_{tag}<{g}> {{\n"
+        f"  static constexpr int N = {len(seeds)};\n"
+        f"  static constexpr int SLOTS = {slots};\n"
+        f"  __host__ __device__ static constexpr int SEED(int k) {{\n"
+        f"    switch (k) {{ {cases} }}\n    return -1;\n  }}\n"
+        f"  template <typename T, typename TF, typename Ctx>\n"
+        f"  __device__ __forceinline__ static void eval(const Ctx &ctx, volatile T *sm) {{\n"
+        f"    {fname}<T, TF>(ctx, sm);\n  }}\n}};\n"
+    )
+
+
+def generate_adjoint(tag: str) -> None:
+    """Reverse-mode point functions of one variant (nrpy_b200/csrc/gen/bssn_adj_<tag>.cuh).
+
+    * a leaf table: one row per gridfunction value and per finite-difference derivative
+      that Ricci, the RHS or H reads (gf, kind, directions), which the stencil-transpose
+      kernel walks;
+    * stencil weights at offsets -3..3 (centred first/second derivative, upwind, KO) and
+      the shifted radiation first-derivative stencils;
+    * VJP functions of the Ricci and RHS output groups, of H and of the detgammabar
+      projection; and the upwind-selector bits of a point.
+    """
+    import sympy as sp
+
+    from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen import fdcoeffs as fdc
+    from nrpy_b200.codegen.emit_cuda import PointKernel
+    from nrpy_b200.codegen.reverse import emit_vjp_function, leaf_table
+
+    coord, sym = VARIANTS[tag]
+    be.setup_nrpy(sym)
+    t0 = time.time()
+    rhs, betaU = be.rhs_exprs(coord)
+    ricci = be.ricci_exprs(coord)
+    cons = be.constraint_exprs(coord)
+    enf = be.enforce_exprs(coord)
+    names = set()
+    for e in list(rhs.values()) + list(ricci.values()) + [cons["H"]]:
+        names |= {x.name for x in sp.sympify(e).free_symbols}
+    rows = leaf_table(sorted(names))
+    row_of = {r[0]: i for i, r in enumerate(rows)}
+    parts = [f"constexpr int adj_nrows_{tag} = {len(rows)};\n",
+             "// leaf rows: {gridfunction, kind (0 value, 1 dD, 2 dDD, 3 dupD, 4 dKOD), dir1, dir2}\n",
+             f"constexpr signed char adj_rows_{tag}[{len(rows)}][4] = {{\n"]
+    parts += [f"    {{{gf}, {kind}, {d1}, {d2}}},  // {name}\n" for name, gf, kind, d1, d2 in rows]
+    parts.append("};\n")
+
+    def wrow(w):
+        return "{" + ", ".join(_c_rational(w.get(s, 0)) for s in range(-3, 4)) + "}"
+
+    up = fdc.upwind(+1)
+    parts.append("// stencil weights at offsets -3..3 (before the invdxx factors)\n")
+    parts.append(f"constexpr double adj_wD_{tag}[7] = {wrow(fdc.first_centred())};\n")
+    parts.append(f"constexpr double adj_wDD_{tag}[7] = {wrow(fdc.second_centred())};\n")
+    parts.append(f"constexpr double adj_wUP_{tag}[7] = {wrow(up)};\n")
+    parts.append(f"constexpr double adj_wKO_{tag}[7] = {wrow(fdc.kreiss_oliger())};\n")
+    fd1 = ", ".join("{" + ", ".join(_c_rational(fdc.radiation_fd1(o).get(s, 0)) for s in range(-4, 5)) + "}"
+                    for o in range(-2, 3))
+    parts.append(f"// radiation first derivative, stencil shift -2..2, offsets -4..4\n"
+                 f"constexpr double adj_wFD1_{tag}[5][9] = {{{fd1}}};\n\n")
+    stats = {}
+    structs = [f"template <int G> struct RicciVjp_{tag};\n", f"template <int G> struct RhsVjp_{tag};\n"]
+    for g, gnames in enumerate(RICCI_GROUPS):
+        fname = f"ricci_vjp_{tag}_g{g}"
+        code, st = emit_vjp_function(fname, [ricci[k] for k in gnames], row_of, symmetry_axes=sym,
+                                     comment=f"VJP of Rbar_ij {gnames} (Ricci_eval.py:27-167)",
+                                     reg_capacity=ADJ_REG_CAPACITY)
+        parts.append(code)
+        stats[f"ricci_g{g}"] = st
+        structs.append(_vjp_struct("RicciVjp", tag, g, fname, [be.RBAR_ORDER.index(k) for k in gnames],
+                                   st["smem_slots"]))
+    for g, gnames in enumerate(RHS_GROUPS):
+        fname = f"rhs_vjp_{tag}_g{g}"
+        code, st = emit_vjp_function(fname, [rhs[k] for k in gnames], row_of, upwind_vec=betaU,
+                                     symmetry_axes=sym, comment=f"VJP of the RHS of {gnames} (rhs_eval.py:122-220)",
+                                     reg_capacity=ADJ_REG_CAPACITY)
+        parts.append(code)
+        stats[f"rhs_g{g}"] = st
+        structs.append(_vjp_struct("RhsVjp", tag, g, fname, [be.GF_ORDER.index(k) for k in gnames],
+                                   st["smem_slots"]))
+    code, st = emit_vjp_function(f"h_vjp_{tag}", [cons["H"]], row_of, symmetry_axes=sym,
+                                 comment="VJP of the Hamiltonian constraint H (constraints_eval.py:364-492)",
+                                 reg_capacity=ADJ_REG_CAPACITY)
+    parts.append(code)
+    stats["H"] = st
+    hnames = ["hDD00", "hDD01", "hDD02", "hDD11", "hDD12", "hDD22"]
+    code, st = emit_vjp_function(f"enforce_vjp_{tag}", [enf[k] for k in hnames], row_of, symmetry_axes=sym,
+                                 comment="VJP of the detgammabar projection "
+                                 "(enforce_detgammabar_equals_detgammahat.py:85-110)",
+                                 reg_capacity=ADJ_REG_CAPACITY)
+    parts.append(code)
+    stats["enforce"] = st
+    pk = PointKernel(sym)
+    pk.upwind_vec = betaU
+    pk._ensure_upwind()
+    body = "\n".join("  " + ln for ln in pk.lines)
+    parts.append(
+        "// Upwind selectors of a point (bit i: betaU[i] = vetU[i]*ReU[i] > 0), the same expressions\n"
+        "// the RHS functions evaluate.\n"
+        f"template <typename T, typename TF, typename Ctx>\n"
+        f"__device__ __forceinline__ int upwind_bits_{tag}(const Ctx &ctx) {{\n{body}\n"
+        "  return (Upwind0 ? 1 : 0) | (Upwind1 ? 2 : 0) | (Upwind2 ? 4 : 0);\n}\n"
+    )
+    hdr = (
+        "// Generated by nrpy_b200/codegen/generate.py (reverse mode, nrpy_b200/codegen/reverse.py).\n"
+        f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}'.\n"
+        f"// Per point: {stats}\n"
+        "#pragma once\n\n"
+    )
+    OUTDIR.mkdir(parents=True, exist_ok=True)
+    (OUTDIR / f"bssn_adj_{tag}.cuh").write_text(hdr + "".join(parts) + "\n" + "\n".join(structs))
+    print(f"adjoint {tag}: {len(rows)} leaf rows, {stats} ({time.time() - t0:.1f}s)")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--variants", default=",".join(VARIANTS))
+    ap.add_argument("--adjoint", default=",".join(ADJOINT_VARIANTS))
     ap.add_argument("--one", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--one-adjoint", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.one:
         generate_variant(args.one)
+        return
+    if args.one_adjoint:
+        generate_adjoint(args.one_adjoint)
         return
     shim = ROOT / "oracle" / "_ref" / "shim"
     env = dict(os.environ)
     env["PYTHONPATH"] = f"{ROOT}:{shim}:{args.reference}"
     procs = [
         subprocess.Popen([sys.executable, "-m", "nrpy_b200.codegen.generate", "--one", tag], env=env, cwd=ROOT)
-        for tag in args.variants.split(",")
+        for tag in args.variants.split(",") if tag
+    ]
+    procs += [
+        subprocess.Popen([sys.executable, "-m", "nrpy_b200.codegen.generate", "--one-adjoint", tag], env=env,
+                         cwd=ROOT)
+        for tag in args.adjoint.split(",") if tag
     ]
     rc = [p.wait() for p in procs]
     if any(rc):

@@ -70,26 +70,6 @@ int launch_inner_bcs(const GridDims &g, const bc_struct *bc, double *gfs, int nu
 }
 
 // ---------------------------------------------------------------- radiation
-// r(xx0) and d(xx0)/dr for the Spherical family (the only nonzero partial x^i / partial r).
-struct RadialMap {
-  int sinh;  // 0: r = xx0 ; 1: r = AMPL sinh(xx0/SINHW)/sinh(1/SINHW)
-  double AMPL, SINHW;
-  __device__ __forceinline__ void eval(double xx0, double &r, double &dx0dr) const {
-    if (!sinh) {
-      r = xx0;
-      dx0dr = 1.0;
-      return;
-    }
-    // Same expression tree as the reference's r_and_partial_xi_partial_r_derivs (SinhSpherical).
-    const double tmp0 = 1.0 / SINHW;
-    const double tmp1 = exp(tmp0) - exp(-tmp0);
-    const double tmp3 = exp(tmp0 * xx0);
-    const double tmp4 = exp(-tmp0 * xx0);
-    r = AMPL * (tmp3 - tmp4) / tmp1;
-    dx0dr = tmp1 / (AMPL * (tmp0 * tmp3 + tmp0 * tmp4));
-  }
-};
-
 // 4th-order first derivative along i0 on a 5-point stencil shifted by `offset` (-2..2),
 // FD1_arbitrary_upwind_x0_dirn of the reference (radiation_BC_fd_order = 4).
 __device__ __forceinline__ double fd1_x0(const double *__restrict__ f, int idx, int offset, double invdx) {
@@ -149,7 +129,7 @@ __global__ void radiation_kernel(const GridDims g, const RadialMap rm, const dou
   rhs[idx + (size_t)gf * g.ntot] = out_here + k * rinv * rinv * rinv;
 }
 
-static int radial_map(const params_struct *p, RadialMap *rm) {
+int radial_map(const params_struct *p, RadialMap *rm) {
   if (p->CoordSystem_hash == SPHERICAL) {
     *rm = RadialMap{0, 0.0, 0.0};
   } else if (p->CoordSystem_hash == SINHSPHERICAL) {

@@ -111,6 +111,28 @@ int launch_rk_points(Variant v, int stage, double dt, const GridDims &g, const R
                      const outerpt_bc_struct *pts, int npts, const double *krhs, cudaStream_t s);
 int launch_rk_substep(int stage, double dt, const GridDims &g, const StageBuffers &b, cudaStream_t s);
 
+// r(xx0) and d(xx0)/dr for the Spherical family (the only nonzero partial x^i / partial r).
+struct RadialMap {
+  int sinh;  // 0: r = xx0 ; 1: r = AMPL sinh(xx0/SINHW)/sinh(1/SINHW)
+  double AMPL, SINHW;
+  __device__ __forceinline__ void eval(double xx0, double &r, double &dx0dr) const {
+    if (!sinh) {
+      r = xx0;
+      dx0dr = 1.0;
+      return;
+    }
+    // Same expression tree as the reference's r_and_partial_xi_partial_r_derivs (SinhSpherical).
+    const double tmp0 = 1.0 / SINHW;
+    const double tmp1 = exp(tmp0) - exp(-tmp0);
+    const double tmp3 = exp(tmp0 * xx0);
+    const double tmp4 = exp(-tmp0 * xx0);
+    r = AMPL * (tmp3 - tmp4) / tmp1;
+    dx0dr = tmp1 / (AMPL * (tmp0 * tmp3 + tmp0 * tmp4));
+  }
+};
+
+int radial_map(const params_struct *p, RadialMap *rm);
+
 // Boundary conditions implemented in boundary.cu.
 int launch_inner_bcs(const GridDims &g, const bc_struct *bc, double *gfs, int num_gfs, const int8_t *parity_types,
                      cudaStream_t s);

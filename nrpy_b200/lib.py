@@ -176,6 +176,14 @@ SIGNATURES = [
     ("bssn_b200_batch_info", C.c_int, [V, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                        C.POINTER(C.c_ulonglong)]),
     ("bssn_b200_batch_destroy", C.c_int, [V]),
+    ("bssn_b200_adjoint_create", C.c_int, [PCD, PGD, C.c_int, C.c_int, V, C.POINTER(V)]),
+    ("bssn_b200_adjoint_forward", C.c_int, [V, C.POINTER(C.c_double)]),
+    ("bssn_b200_adjoint_backward", C.c_int, [V, C.c_double, PR, C.POINTER(C.c_double)]),
+    ("bssn_b200_adjoint_functional", C.c_int, [V, PR, C.POINTER(C.c_double)]),
+    ("bssn_b200_adjoint_functional_vjp", C.c_int, [V, PR, C.c_double, PR]),
+    ("bssn_b200_adjoint_step_vjp", C.c_int, [V, PR, PR]),
+    ("bssn_b200_adjoint_id_vjp", C.c_int, [V, PR, C.POINTER(C.c_double)]),
+    ("bssn_b200_adjoint_destroy", C.c_int, [V]),
     ("bssn_b200_memcpy", C.c_int, [V, V, C.c_size_t, C.c_int]),
     ("bssn_b200_device_synchronize", C.c_int, []),
 ]
