@@ -193,6 +193,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--no-diff", action="store_true", help="skip the adjoint-gradient section")
     ap.add_argument("--nxx", default=None, help="override the grid, e.g. 256,64,32 (profiling only)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -275,6 +276,7 @@ def main():
     del grid, y0, y_fp64
     torch.cuda.empty_cache()
     batched = None if args.no_batched else run_batched(args, world, rank, dist)
+    differentiation = None if (args.no_diff or rank != 0) else run_differentiation()
 
     if rank == 0:
         cpu = None
@@ -308,6 +310,7 @@ def main():
             "cpu_baseline": cpu,
             "mixed": mixed,
             "batched": batched,
+            "differentiation": differentiation,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -408,6 +411,50 @@ def run_batched(args, world, rank, dist):
             "interior_points": pts if dist is None else None, "tile": list(tune["tile"]), "blocks": tune["blocks"],
             "autotune": tune["table"], "graph_kernel_nodes_per_replay": info["kernel_nodes"],
             "sequential_single_grid_value": seq_value, "speedup_vs_sequential": value / seq_value}
+
+
+def run_differentiation(fd_check: bool = True):
+    """Adjoint gradient dJ/d(m1, z1, m2, z2) of J = sum_interior H^2 + alpha(centre) after 200
+    FP64 RK4 steps on Spherical 128x32x32 (checkpoints every 20), timed forward and backward
+    (CUDA events on the grid's stream), checked against central differences (h = 1e-6) of
+    the forward."""
+    import torch
+
+    from nrpy_b200.adjoint import BLGradient, differentiation_workload
+
+    w = differentiation_workload(seed=2024)
+    p = BLGradient(Nxx=w["Nxx"], grid_physical_size=w["grid_physical_size"], nsteps=w["nsteps"],
+                   checkpoint_every=w["checkpoint_every"], theta=w["theta"])
+    p.value_and_grad(w["theta"])  # warm-up
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    J = p.forward(w["theta"])
+    ev[1].record(stream)
+    grad = p.backward(1.0)
+    ev[2].record(stream)
+    ev[2].synchronize()
+    ms_f, ms_b = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    res = {"workload": "Spherical 128x32x32 (+3 ghosts), grid_physical_size 7.5, 200 FP64 RK4 steps, radiation BCs, "
+                       "checkpoints every 20; J = sum_interior H^2 + alpha(NGHOSTS, N1/2, N2/2)",
+           "theta_names": ["BH1_mass", "BH1_posn_z", "BH2_mass", "BH2_posn_z"], "theta": list(w["theta"]),
+           "seed": w["seed"], "J": J["J"], "grad": [float(x) for x in grad], "ms_forward": ms_f,
+           "ms_backward": ms_b, "backward_over_forward": ms_b / ms_f,
+           "pt_updates_per_s_forward": p.grid.n_interior * w["nsteps"] / (ms_f * 1e-3),
+           "pt_updates_per_s_backward": p.grid.n_interior * w["nsteps"] / (ms_b * 1e-3)}
+    if fd_check:
+        h = 1e-6
+        fd = []
+        for k in range(4):
+            tp, tm = list(w["theta"]), list(w["theta"])
+            tp[k] += h
+            tm[k] -= h
+            fd.append((p.forward(tp)["J"] - p.forward(tm)["J"]) / (2 * h))
+        res["central_fd_h"] = h
+        res["central_fd"] = fd
+        res["rel_err_vs_fd"] = [abs(a - b) / abs(b) for a, b in zip(grad, fd)]
+    p.close()
+    return res
 
 
 def time_fused_kernel(grid, lib, stream, reps: int = 5):
