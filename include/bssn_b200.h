@@ -317,7 +317,7 @@ int bssn_b200_stepper_kernel_nodes(const bssn_b200_stepper *st, unsigned long lo
  * grid, rfm, bcstruct, storage, initial data; all of one coordinate system, full 3-D,
  * radiation outer BCs; each with its own commondata: masses, dt, ...) advanced together.
  * Each RK4 stage of the whole batch takes a fixed number of launches: persistent kernels
- * (`blocks` CTAs of tile_bx x tile_by = 128 threads) walk one tile list over all grids.
+ * (`blocks` CTAs) walk one tile list over all grids; a tile is tile_bx x tile_by = 128 points.
  * `steps_per_graph` RK4 steps are captured into a CUDA graph on `stream` (non-default);
  * bssn_b200_batch_run replays it. Creation allocates the per-grid RHS shells and the
  * device work lists; the caller's states are unchanged by it. */

@@ -423,23 +423,28 @@ def _parse(lines: List[str]):
     return out
 
 
-def _is_remat(ty: str, rhs: str, remat: Dict[str, str]) -> bool:
+def _is_remat(ty: str, rhs: str, remat: Dict[str, str], deriv_remat: bool = False) -> bool:
     if ty == "double" and rhs.startswith("LD("):
         return True
     if ty == "T" and (rhs.startswith("T(RFM(") or rhs.startswith("T(PARAM(") or rhs.startswith("T(LDAUX(")):
         return True
+    if deriv_remat and ty == "T" and rhs.startswith("T(TF(invdxx"):
+        return True  # finite difference: recomputed from its stencil loads at each use
     m = re.fullmatch(r"T\((v_\w+)\)", rhs)
     return bool(m and m.group(1) in remat)
 
 
-def allocate_values(lines: List[str], reg_capacity: int) -> Tuple[List[str], int]:
+def allocate_values(lines: List[str], reg_capacity: int, remat_first: bool = False,
+                    deriv_remat: bool = False) -> Tuple[List[str], int]:
     """Keep at most `reg_capacity` values in registers at any statement.
 
-    Linear scan over live intervals (Poletto-Sarkar): when too many values are live, the
-    one whose interval ends last leaves the register set. Values that are plain loads
-    (stencil points, rfm arrays, parameters) are re-read at each use instead; all others
-    are stored once to a per-thread shared-memory slot, SMEM(k), and read from it at each
-    use (the slot array is volatile, so the compiler cannot keep the value in a register).
+    Linear scan over live intervals (Poletto-Sarkar): when too many values are live, one
+    leaves the register set -- the one whose interval ends last, or with `remat_first` the
+    furthest-ending value that can be recomputed from memory (stencil loads, rfm arrays,
+    parameters, and with `deriv_remat` finite differences) if any is live. Recomputable
+    values are re-read (re-evaluated) at each use; all others are stored once to a
+    per-thread shared-memory slot, SMEM(k), and read from it at each use (the slot array is
+    volatile, so the compiler cannot keep the value in a register).
     Returns the rewritten statements and the number of shared-memory slots.
     """
     st = _parse(lines)
@@ -450,10 +455,14 @@ def allocate_values(lines: List[str], reg_capacity: int) -> Tuple[List[str], int
         for t in _TOK_RE.findall(rhs):
             if t in idx:
                 last[t] = i
-    remat: Dict[str, str] = {}
+    remat: Dict[str, str] = {}  # name -> expression in loads / rfm / parameters only
+
+    def expand(rhs: str) -> str:
+        return _TOK_RE.sub(lambda m: f"({remat[m.group(0)]})" if m.group(0) in remat else m.group(0), rhs)
+
     for name, ty, rhs, is_out in st:
-        if not is_out and _is_remat(ty, rhs, remat):
-            remat[name] = rhs
+        if not is_out and _is_remat(ty, rhs, remat, deriv_remat):
+            remat[name] = expand(rhs)
     # intervals of values that need storage (bools stay in registers: predicates)
     iv = [(idx[v], last.get(v, idx[v]), v) for v in idx if st[idx[v]][1] != "bool"]
     iv.sort()
@@ -465,7 +474,14 @@ def allocate_values(lines: List[str], reg_capacity: int) -> Tuple[List[str], int
         active = [(e, a) for e, a in active if e > start]  # intervals ending at start are done
         bisect.insort(active, (end, v))
         if len(active) > reg_capacity:
-            e, victim = active.pop()  # furthest end
+            victim = None
+            if remat_first:
+                for k in range(len(active) - 1, -1, -1):
+                    if active[k][1] in remat:
+                        victim = active.pop(k)[1]
+                        break
+            if victim is None:
+                victim = active.pop()[1]  # furthest end
             spilled[victim] = True
     # shared-memory slots for spilled, non-rematerializable values (interval colouring)
     slot_of: Dict[str, int] = {}
@@ -496,11 +512,7 @@ def allocate_values(lines: List[str], reg_capacity: int) -> Tuple[List[str], int
             t = m.group(0)
             if t in spilled:
                 if t in remat:
-                    r = remat[t]
-                    inner = re.fullmatch(r"T\((v_\w+)\)", r)
-                    if inner and inner.group(1) in remat:
-                        return f"T({remat[inner.group(1)]})"
-                    return f"({r})"
+                    return f"({remat[t]})"
                 return f"SMEM({slot_of[t]})"
             return t
 
@@ -527,18 +539,22 @@ def emit_point_function(
     symmetry_axes: str = "",
     comment: str = "",
     reg_capacity: int = 0,
+    remat_first: bool = False,
+    deriv_remat: bool = False,
 ) -> Tuple[str, Dict[str, int]]:
     """Emit `fname` and the constant `fname_SMEM_SLOTS`. With reg_capacity > 0 the values
     beyond that many live doubles go to shared-memory slots (SMEM(k), provided by the
-    caller through the `sm` argument: slot k of this thread)."""
+    caller through the `sm` argument: slot k of this thread; the template parameter NT is
+    the slot stride, i.e. the threads of a block)."""
     pk = PointKernel(symmetry_axes)
     pk.build(outputs, upwind_vec)
-    lines, nslots = (allocate_values(dfs_order(pk.lines), reg_capacity) if reg_capacity > 0 else (pk.lines, 0))
+    lines, nslots = (allocate_values(dfs_order(pk.lines), reg_capacity, remat_first, deriv_remat)
+                     if reg_capacity > 0 else (pk.lines, 0))
     body = "\n".join("  " + ln for ln in lines)
     head = f"// {comment}\n" if comment else ""
     code = (
         f"{head}constexpr int {fname}_SMEM_SLOTS = {nslots};\n"
-        f"template <typename T, typename TF, typename Ctx>\n"
+        f"template <typename T, typename TF, int NT = 128, typename Ctx>\n"
         f"__device__ __forceinline__ void {fname}(const Ctx &ctx, T *__restrict__ out, volatile T *sm) {{\n"
         f"  (void)sm;\n{body}\n}}\n"
     )

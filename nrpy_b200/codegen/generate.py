@@ -16,7 +16,7 @@ import sys
 import time
 
 ROOT = pathlib.Path(__file__).resolve().parents[2]
-OUTDIR = ROOT / "nrpy_b200" / "csrc" / "gen"
+OUTDIR = pathlib.Path(os.environ.get("BSSN_GEN_OUTDIR", str(ROOT / "nrpy_b200" / "csrc" / "gen")))
 VARIANTS = {
     # tag: (CoordSystem, symmetry_axes)
     "sph_axi": ("Spherical", "2"),
@@ -36,6 +36,21 @@ RHS_GROUPS = [
     ["betU0", "betU1", "betU2", "lambdaU0", "lambdaU1", "lambdaU2"],
 ]
 REG_CAPACITY = 90
+# Per group: (remat_first, deriv_remat) of the value allocator -- whether register eviction
+# prefers recomputable values (stencil loads, rfm, parameters) and whether finite
+# differences are recomputed from their stencils instead of kept in a slot. Chosen by
+# timing every group kernel of SinhSpherical 256x64x32 on a B200 under each allocation
+# (and 64/128 threads per block); lower register budgets with forced occupancy were
+# slower in every group (local-memory spills).
+RICCI_ALLOC = [(True, True), (True, True), (True, True)]
+RHS_ALLOC = [(False, False), (True, False), (True, False)]
+# Threads per block of a group kernel: 128, or 64 when two 128-thread blocks of its
+# shared-memory slots would not fit in the 227 KB of one SM.
+SMEM_PER_SM = 227 * 1024
+
+
+def threads_for(slots: int) -> int:
+    return 128 if 2 * slots * 8 * 128 <= SMEM_PER_SM else 64
 # Reverse-mode (adjoint) functions: generated for these variants only; fewer values in
 # registers because the VJP kernels run 64 threads per block with shared-memory slots.
 ADJOINT_VARIANTS = ["sph_3d"]
@@ -48,11 +63,12 @@ def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int) -> s
         f"template <> struct {kind}_{tag}<{g}> {{\n"
         f"  static constexpr int N = {len(gfs)};\n"
         f"  static constexpr int SLOTS = {slots};\n"
+        f"  static constexpr int NT = {threads_for(slots)};  // threads per block of the single-grid kernels\n"
         f"  __host__ __device__ static constexpr int GF(int k) {{\n"
         f"    switch (k) {{ {cases} }}\n    return -1;\n  }}\n"
-        f"  template <typename T, typename TF, typename Ctx>\n"
+        f"  template <typename T, typename TF, int NTB, typename Ctx>\n"
         f"  __device__ __forceinline__ static void eval(const Ctx &ctx, T *out, volatile T *sm) {{\n"
-        f"    {fname}<T, TF>(ctx, out, sm);\n  }}\n}};\n"
+        f"    {fname}<T, TF, NTB>(ctx, out, sm);\n  }}\n}};\n"
     )
 
 
@@ -72,10 +88,11 @@ def generate_variant(tag: str) -> None:
     structs = [f"template <int G> struct RicciGroup_{tag};\n", f"template <int G> struct RhsGroup_{tag};\n"]
     for g, names in enumerate(RICCI_GROUPS):
         fname = f"ricci_point_{tag}_g{g}"
+        remat_first, deriv_remat = RICCI_ALLOC[g]
         code, st = emit_point_function(
             fname, [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
             comment=f"Rbar_ij {names}, {coord} (symmetry_axes='{sym}'): Ricci_eval.py:27-167",
-            reg_capacity=REG_CAPACITY,
+            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat,
         )
         parts.append(code)
         stats[f"ricci_g{g}"] = st
@@ -83,10 +100,11 @@ def generate_variant(tag: str) -> None:
                                      st["smem_slots"]))
     for g, names in enumerate(RHS_GROUPS):
         fname = f"rhs_point_{tag}_g{g}"
+        remat_first, deriv_remat = RHS_ALLOC[g]
         code, st = emit_point_function(
             fname, [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU, symmetry_axes=sym,
             comment=f"BSSN RHS + KO (CAKO) of {names}, {coord} (symmetry_axes='{sym}'): rhs_eval.py:122-220",
-            reg_capacity=REG_CAPACITY,
+            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat,
         )
         parts.append(code)
         stats[f"rhs_g{g}"] = st
@@ -122,6 +140,8 @@ def generate_variant(tag: str) -> None:
     hdr = (
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', 4th-order FD, KO (CAKO).\n"
+        f"// Register budget {REG_CAPACITY} values; allocation (remat_first, deriv_remat): Ricci {RICCI_ALLOC}, "
+        f"RHS {RHS_ALLOC}.\n"
         f"// Per point: {stats}\n"
         "#pragma once\n\n"
     )

@@ -179,7 +179,7 @@ int bssn_b200_batch_create(int nevo, commondata_struct *const *cds, griddata_str
   }
   if (tile_bx * tile_by != 128 || tile_bx < 1 || tile_by < 1 || blocks < 1 || steps_per_graph < 1 ||
       steps_per_graph > 1000) {
-    set_error("batch: tile %dx%d must have 128 threads; blocks >= 1; 1 <= steps_per_graph <= 1000", tile_bx,
+    set_error("batch: tile %dx%d must have 128 points; blocks >= 1; 1 <= steps_per_graph <= 1000", tile_bx,
               tile_by);
     return BSSN_B200_EINVAL;
   }

@@ -57,7 +57,8 @@ struct RegCtx {
 #define rfm_f1_DD11 f1_DD11
 #define PARAM(name) ctx.name
 // Per-thread shared-memory slot k (the kernel passes `sm` already offset by its thread).
-#define SMEM(k) sm[(k) * (BX * BY)]
+// NT is the slot stride: the template parameter of the generated function (threads per block).
+#define SMEM(k) sm[(k) * NT]
 #define invdxx0 ctx.invdxx0
 #define invdxx1 ctx.invdxx1
 #define invdxx2 ctx.invdxx2
@@ -113,14 +114,14 @@ __device__ __forceinline__ PointCtx make_ctx(const GridDims &g, const RfmArrays 
   return c;
 }
 
-static dim3 interior_grid(const GridDims &g) {
+static dim3 interior_grid(const GridDims &g, int by = BY) {
   const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
-  return dim3((n0 + BX - 1) / BX, (n1 + BY - 1) / BY, n2);
+  return dim3((n0 + BX - 1) / BX, (n1 + by - 1) / by, n2);
 }
 
 #define INTERIOR_INDEX_OR_RETURN(g)                       \
   const int i0 = NGHOSTS + blockIdx.x * BX + threadIdx.x; \
-  const int i1 = NGHOSTS + blockIdx.y * BY + threadIdx.y; \
+  const int i1 = NGHOSTS + blockIdx.y * blockDim.y + threadIdx.y; \
   const int i2 = NGHOSTS + blockIdx.z;                    \
   if (i0 >= g.N0 - NGHOSTS || i1 >= g.N1 - NGHOSTS) return;
 
@@ -130,28 +131,28 @@ __device__ __forceinline__ volatile T *thread_slots() {
   return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + blockDim.x * threadIdx.y);
 }
 
-template <Variant V, int G, typename T = double>
+template <Variant V, int G, typename T, int NTB>
 __device__ __forceinline__ void ricci_body(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux,
                                            int i0, int i1, int i2, volatile T *sm) {
   using Grp = RicciG<V, G>;
   const PointCtx ctx = make_ctx(g, rfm, in, nullptr, i0, i1, i2);
   T out[Grp::N];
-  Grp::template eval<T, double>(ctx, out, sm);
+  Grp::template eval<T, double, NTB>(ctx, out, sm);
   const int idx = i0 + g.s1 * i1 + g.s2 * i2;
 #pragma unroll
   for (int k = 0; k < Grp::N; k++) aux[idx + Grp::GF(k) * g.ntot] = double(out[k]);
 }
 
 template <Variant V, int G, typename T>
-__global__ void __launch_bounds__(BX *BY, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
+__global__ void __launch_bounds__(RicciG<V, G>::NT, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
                                                           const double *__restrict__ in, double *__restrict__ aux) {
   volatile T *sm = thread_slots<T>();
   INTERIOR_INDEX_OR_RETURN(g);
-  ricci_body<V, G, T>(g, rfm, in, aux, i0, i1, i2, sm);
+  ricci_body<V, G, T, RicciG<V, G>::NT>(g, rfm, in, aux, i0, i1, i2, sm);
 }
 
 template <Variant V, typename T, int G>
-__global__ void __launch_bounds__(BX *BY, 1) rhs_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
+__global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
                                                         const double *__restrict__ aux, const double *__restrict__ in,
                                                         double *__restrict__ rhs) {
   using Grp = RhsG<V, G>;
@@ -162,7 +163,7 @@ __global__ void __launch_bounds__(BX *BY, 1) rhs_kernel(const GridDims g, const 
   ctx.KreissOliger_strength_gauge = pp.ko_gauge;
   ctx.KreissOliger_strength_nongauge = pp.ko_nongauge;
   T out[Grp::N];
-  Grp::template eval<T, double>(ctx, out, sm);
+  Grp::template eval<T, double, Grp::NT>(ctx, out, sm);
   const int idx = i0 + g.s1 * i1 + g.s2 * i2;
 #pragma unroll
   for (int k = 0; k < Grp::N; k++) rhs[idx + Grp::GF(k) * g.ntot] = double(out[k]);
@@ -255,7 +256,7 @@ __device__ __forceinline__ void rk_and_project_point(const GridDims &g, const Rf
 // of that group's gridfunctions; the group holding hDD also applies the detgammabar
 // projection to the new hDD. The raw RHS is also stored to `krhs` on the interior shell
 // (the layer next to each face), where the outer radiation condition reads it.
-template <Variant V, typename T, int STAGE, int G>
+template <Variant V, typename T, int STAGE, int G, int NTB>
 __device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
                                            const double *aux, const StageBuffers &b, double *krhs, const double dt,
                                            int i0, int i1, int i2, volatile T *sm) {
@@ -265,7 +266,7 @@ __device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &r
   ctx.KreissOliger_strength_gauge = pp.ko_gauge;
   ctx.KreissOliger_strength_nongauge = pp.ko_nongauge;
   T kt[Grp::N];
-  Grp::template eval<T, double>(ctx, kt, sm);
+  Grp::template eval<T, double, NTB>(ctx, kt, sm);
   const int idx = i0 + g.s1 * i1 + g.s2 * i2;
   const bool shell = (i0 == NGHOSTS) | (i0 == g.N0 - NGHOSTS - 1) | (i1 == NGHOSTS) | (i1 == g.N1 - NGHOSTS - 1) |
                      (i2 == NGHOSTS) | (i2 == g.N2 - NGHOSTS - 1);
@@ -300,12 +301,12 @@ __device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &r
 // projection to the new hDD. The raw RHS is also stored to `krhs` on the interior shell
 // (the layer next to each face), where the outer radiation condition reads it.
 template <Variant V, typename T, int STAGE, int G>
-__global__ void __launch_bounds__(BX *BY, 1) rhs_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
+__global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
                                                               const double *__restrict__ aux, const StageBuffers b,
                                                               double *__restrict__ krhs, const double dt) {
   volatile T *sm = thread_slots<T>();
   INTERIOR_INDEX_OR_RETURN(g);
-  fused_body<V, T, STAGE, G>(g, rfm, pp, aux, b, krhs, dt, i0, i1, i2, sm);
+  fused_body<V, T, STAGE, G, RhsG<V, G>::NT>(g, rfm, pp, aux, b, krhs, dt, i0, i1, i2, sm);
 }
 
 // RK update plus projection of listed boundary points whose RHS is already in krhs.
@@ -337,10 +338,10 @@ static bool empty_interior(const GridDims &g) {
   return g.N0 <= 2 * NGHOSTS || g.N1 <= 2 * NGHOSTS || g.N2 <= 2 * NGHOSTS;
 }
 
-// Dynamic shared memory of a group kernel: SLOTS values of type T per thread.
+// Dynamic shared memory of a group kernel: SLOTS values of type T for each of its NT threads.
 template <typename Grp, typename T>
 constexpr size_t slot_bytes() {
-  return (size_t)Grp::SLOTS * BX * BY * sizeof(T);
+  return (size_t)Grp::SLOTS * Grp::NT * sizeof(T);
 }
 
 template <typename KernelPtr>
@@ -354,7 +355,7 @@ static int launch_ricci_group(const GridDims &g, const RfmArrays &rfm, const dou
   using Grp = RicciG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(ricci_kernel<V, G, T>, sb));
-  ricci_kernel<V, G, T><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, in, aux);
+  ricci_kernel<V, G, T><<<interior_grid(g, Grp::NT / BX), dim3(BX, Grp::NT / BX), sb, s>>>(g, rfm, in, aux);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -384,7 +385,7 @@ static int launch_rhs_group(const GridDims &g, const RfmArrays &rfm, const PhysP
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(rhs_kernel<V, T, G>, sb));
-  rhs_kernel<V, T, G><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, pp, aux, in, rhs);
+  rhs_kernel<V, T, G><<<interior_grid(g, Grp::NT / BX), dim3(BX, Grp::NT / BX), sb, s>>>(g, rfm, pp, aux, in, rhs);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -438,7 +439,8 @@ static int launch_fused_group(const GridDims &g, const RfmArrays &rfm, const Phy
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(rhs_fused_kernel<V, T, STAGE, G>, sb));
-  rhs_fused_kernel<V, T, STAGE, G><<<interior_grid(g), dim3(BX, BY), sb, s>>>(g, rfm, pp, aux, b, krhs, dt);
+  rhs_fused_kernel<V, T, STAGE, G><<<interior_grid(g, Grp::NT / BX), dim3(BX, Grp::NT / BX), sb, s>>>(g, rfm, pp, aux, b,
+                                                                                              krhs, dt);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -503,47 +505,57 @@ int launch_rk_points(Variant v, int stage, double dt, const GridDims &g, const R
 // ---------------------------------------------------------------- batched evolutions
 // Persistent kernels over a tile list that spans every evolution of a batch: block b takes
 // tiles b, b + gridDim.x, ... Tile t belongs to evolution tile_evo[t]; its local index runs
-// over (tiles_x, tiles_y, n2) tiles of blockDim.x x blockDim.y interior points.
-__device__ __forceinline__ bool tile_point(const EvoDesc &d, int t_local, int &i0, int &i1, int &i2) {
+// over (tiles_x, tiles_y, n2) tiles of bx x by = 128 interior points. A block has the
+// group's NT threads (1-D) and covers a tile in 128 / NT passes.
+__device__ __forceinline__ bool tile_point(const EvoDesc &d, int t_local, int lin, int bx, int by, int &i0, int &i1,
+                                           int &i2) {
   const int tx = t_local % d.tiles_x;
   const int r = t_local / d.tiles_x;
   const int ty = r % d.tiles_y;
   const int tz = r / d.tiles_y;
-  i0 = NGHOSTS + tx * blockDim.x + threadIdx.x;
-  i1 = NGHOSTS + ty * blockDim.y + threadIdx.y;
+  i0 = NGHOSTS + tx * bx + lin % bx;
+  i1 = NGHOSTS + ty * by + lin / bx;
   i2 = NGHOSTS + tz;
   return i0 < d.g.N0 - NGHOSTS && i1 < d.g.N1 - NGHOSTS;
 }
 
 template <Variant V, int G>
-__global__ void __launch_bounds__(BX *BY, 1) ricci_batched_kernel(const EvoDesc *__restrict__ descs,
-                                                                  const int *__restrict__ tile_evo, const int ntiles,
-                                                                  const int stage) {
+__global__ void __launch_bounds__(RicciG<V, G>::NT, 1) ricci_batched_kernel(const EvoDesc *__restrict__ descs,
+                                                                          const int *__restrict__ tile_evo,
+                                                                          const int ntiles, const int stage,
+                                                                          const int bx, const int by) {
+  constexpr int NT = RicciG<V, G>::NT;
   volatile double *sm = thread_slots<double>();
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const EvoDesc &d = descs[tile_evo[t]];
-    int i0, i1, i2;
-    if (!tile_point(d, t - d.tile_begin, i0, i1, i2)) continue;
     double *kin, *kout;
     stage_io(d, stage, kin, kout);
-    ricci_body<V, G, double>(d.g, d.rfm, kin, d.aux, i0, i1, i2, sm);
+    for (int pass = 0; pass < (BX * BY) / NT; pass++) {
+      int i0, i1, i2;
+      if (!tile_point(d, t - d.tile_begin, pass * NT + threadIdx.x, bx, by, i0, i1, i2)) continue;
+      ricci_body<V, G, double, NT>(d.g, d.rfm, kin, d.aux, i0, i1, i2, sm);
+    }
   }
 }
 
 template <Variant V, int STAGE, int G>
-__global__ void __launch_bounds__(BX *BY, 1) rhs_fused_batched_kernel(const EvoDesc *__restrict__ descs,
-                                                                      const int *__restrict__ tile_evo,
-                                                                      const int ntiles) {
+__global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_fused_batched_kernel(const EvoDesc *__restrict__ descs,
+                                                                            const int *__restrict__ tile_evo,
+                                                                            const int ntiles, const int bx,
+                                                                            const int by) {
+  constexpr int NT = RhsG<V, G>::NT;
   volatile double *sm = thread_slots<double>();
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const EvoDesc &d = descs[tile_evo[t]];
-    int i0, i1, i2;
-    if (!tile_point(d, t - d.tile_begin, i0, i1, i2)) continue;
     StageBuffers b;
     b.y = d.y;
     b.run = d.run;
     stage_io(d, STAGE, b.kin, b.kout);
-    fused_body<V, double, STAGE, G>(d.g, d.rfm, d.pp, d.aux, b, d.krhs, d.dt, i0, i1, i2, sm);
+    for (int pass = 0; pass < (BX * BY) / NT; pass++) {
+      int i0, i1, i2;
+      if (!tile_point(d, t - d.tile_begin, pass * NT + threadIdx.x, bx, by, i0, i1, i2)) continue;
+      fused_body<V, double, STAGE, G, NT>(d.g, d.rfm, d.pp, d.aux, b, d.krhs, d.dt, i0, i1, i2, sm);
+    }
   }
 }
 
@@ -571,7 +583,8 @@ static int launch_ricci_batched_group(int stage, const EvoDesc *descs, const int
   using Grp = RicciG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, double>();
   BSSN_TRY(set_smem(ricci_batched_kernel<V, G>, sb));
-  ricci_batched_kernel<V, G><<<blocks, dim3(bx, by), sb, s>>>(descs, tile_evo, ntiles, stage);
+  // `blocks` counts 128-thread CTAs; a group with fewer threads per CTA gets proportionally more.
+  ricci_batched_kernel<V, G><<<blocks * (BX * BY / Grp::NT), Grp::NT, sb, s>>>(descs, tile_evo, ntiles, stage, bx, by);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -582,7 +595,8 @@ static int launch_fused_batched_group(const EvoDesc *descs, const int *tile_evo,
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, double>();
   BSSN_TRY(set_smem(rhs_fused_batched_kernel<V, STAGE, G>, sb));
-  rhs_fused_batched_kernel<V, STAGE, G><<<blocks, dim3(bx, by), sb, s>>>(descs, tile_evo, ntiles);
+  rhs_fused_batched_kernel<V, STAGE, G><<<blocks * (BX * BY / Grp::NT), Grp::NT, sb, s>>>(descs, tile_evo, ntiles, bx,
+                                                                                        by);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -597,7 +611,7 @@ static int launch_fused_batched_stage(const EvoDesc *descs, const int *tile_evo,
 
 static int check_shape(int bx, int by) {
   if (bx * by != BX * BY || bx < 1 || by < 1) {
-    set_error("batched tile shape %dx%d: must have %d threads", bx, by, BX * BY);
+    set_error("batched tile shape %dx%d: must have %d points", bx, by, BX * BY);
     return BSSN_B200_EINVAL;
   }
   return BSSN_B200_OK;
