@@ -295,7 +295,7 @@ def main():
                        "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",
                        "parallelism": f"replicas x{world}", "seed": args.seed, "bl": [m1, z1, m2, z2],
                        "dt": grid_dt, "H_L2_last": h_hist[-1] if h_hist else None},
-            "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel, groups 0-2 (one interior RK stage: RHS + RK4 update + projection)",
+            "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel, all output groups (one interior RK stage: RHS + RK4 update + projection)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
                          "traffic": profiled_traffic() if NXX == (256, 64, 64) else None,

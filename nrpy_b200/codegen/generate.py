@@ -28,9 +28,18 @@ VARIANTS = {
 
 # Output groups: each group is one kernel (its own CSE); groups trade recomputed shared
 # subexpressions for fewer live values per thread. Values beyond REG_CAPACITY live doubles
-# go to per-thread shared-memory slots.
-RICCI_GROUPS = [["RbarDD00", "RbarDD01"], ["RbarDD02", "RbarDD11"], ["RbarDD12", "RbarDD22"]]
+# go to per-thread shared-memory slots. The split was chosen by timing every candidate
+# group kernel of SinhSpherical 256x64x32 on a B200 (Ricci: 1x6, 2x3, 3x2 and 6x1 outputs;
+# RHS: the gauge/metric/extrinsic-curvature outputs together or in two or three parts).
+RICCI_GROUPS = [["RbarDD00", "RbarDD01", "RbarDD02"], ["RbarDD11", "RbarDD12", "RbarDD22"]]
 RHS_GROUPS = [
+    ["aDD00", "aDD01", "aDD02", "aDD11", "aDD12", "aDD22", "alpha", "cf", "hDD00", "hDD01", "hDD02", "hDD11",
+     "hDD12", "hDD22", "trK", "vetU0", "vetU1", "vetU2"],
+    ["betU0", "betU1", "betU2", "lambdaU0", "lambdaU1", "lambdaU2"],
+]
+# The reverse-mode functions keep their own (smaller) groups.
+ADJ_RICCI_GROUPS = [["RbarDD00", "RbarDD01"], ["RbarDD02", "RbarDD11"], ["RbarDD12", "RbarDD22"]]
+ADJ_RHS_GROUPS = [
     ["aDD00", "aDD01", "aDD02", "aDD11", "aDD12", "aDD22"],
     ["alpha", "cf", "hDD00", "hDD01", "hDD02", "hDD11", "hDD12", "hDD22", "trK", "vetU0", "vetU1", "vetU2"],
     ["betU0", "betU1", "betU2", "lambdaU0", "lambdaU1", "lambdaU2"],
@@ -42,8 +51,8 @@ REG_CAPACITY = 90
 # timing every group kernel of SinhSpherical 256x64x32 on a B200 under each allocation
 # (and 64/128 threads per block); lower register budgets with forced occupancy were
 # slower in every group (local-memory spills).
-RICCI_ALLOC = [(True, True), (True, True), (True, True)]
-RHS_ALLOC = [(False, False), (True, False), (True, False)]
+RICCI_ALLOC = [(True, True), (True, True)]
+RHS_ALLOC = [(True, False), (True, False)]
 # Threads per block of a group kernel: 128, or 64 when two 128-thread blocks of its
 # shared-memory slots would not fit in the 227 KB of one SM.
 SMEM_PER_SM = 227 * 1024
@@ -137,6 +146,8 @@ def generate_variant(tag: str) -> None:
     )
     parts.append(code)
     stats["lambda"] = st
+    structs.append(f"constexpr int ricci_group_count_{tag} = {len(RICCI_GROUPS)};\n"
+                   f"constexpr int rhs_group_count_{tag} = {len(RHS_GROUPS)};\n")
     hdr = (
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', 4th-order FD, KO (CAKO).\n"
@@ -222,7 +233,7 @@ def generate_adjoint(tag: str) -> None:
                  f"constexpr double adj_wFD1_{tag}[5][9] = {{{fd1}}};\n\n")
     stats = {}
     structs = [f"template <int G> struct RicciVjp_{tag};\n", f"template <int G> struct RhsVjp_{tag};\n"]
-    for g, gnames in enumerate(RICCI_GROUPS):
+    for g, gnames in enumerate(ADJ_RICCI_GROUPS):
         fname = f"ricci_vjp_{tag}_g{g}"
         code, st = emit_vjp_function(fname, [ricci[k] for k in gnames], row_of, symmetry_axes=sym,
                                      comment=f"VJP of Rbar_ij {gnames} (Ricci_eval.py:27-167)",
@@ -231,7 +242,7 @@ def generate_adjoint(tag: str) -> None:
         stats[f"ricci_g{g}"] = st
         structs.append(_vjp_struct("RicciVjp", tag, g, fname, [be.RBAR_ORDER.index(k) for k in gnames],
                                    st["smem_slots"]))
-    for g, gnames in enumerate(RHS_GROUPS):
+    for g, gnames in enumerate(ADJ_RHS_GROUPS):
         fname = f"rhs_vjp_{tag}_g{g}"
         code, st = emit_vjp_function(fname, [rhs[k] for k in gnames], row_of, upwind_vec=betaU,
                                      symmetry_axes=sym, comment=f"VJP of the RHS of {gnames} (rhs_eval.py:122-220)",

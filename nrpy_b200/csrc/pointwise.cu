@@ -83,7 +83,22 @@ using RhsG = std::conditional_t<
     V == SPH_3D, RhsGroup_sph_3d<G>,
     std::conditional_t<V == SPH_AXI, RhsGroup_sph_axi<G>,
                        std::conditional_t<V == SINH_3D, RhsGroup_sinh_3d<G>, RhsGroup_sinh_axi<G>>>>;
-constexpr int kRicciGroups = 3, kRhsGroups = 3;
+constexpr int kRicciGroups = ricci_group_count_sph_3d, kRhsGroups = rhs_group_count_sph_3d;
+static_assert(ricci_group_count_sph_axi == kRicciGroups && ricci_group_count_sinh_3d == kRicciGroups &&
+                  ricci_group_count_sinh_axi == kRicciGroups && rhs_group_count_sph_axi == kRhsGroups &&
+                  rhs_group_count_sinh_3d == kRhsGroups && rhs_group_count_sinh_axi == kRhsGroups,
+              "every variant has the same output groups");
+
+// Calls f(std::integral_constant<int, G>) for G = G0 .. NG-1, stopping at the first error.
+template <int G0, int NG, typename F>
+static int for_each_group(F &&f) {
+  if constexpr (G0 < NG) {
+    BSSN_TRY(f(std::integral_constant<int, G0>{}));
+    return for_each_group<G0 + 1, NG>(f);
+  } else {
+    return BSSN_B200_OK;
+  }
+}
 
 #define DISPATCH_POINT(NAME, V, T, TF, CTX, OUT)                                  \
   do {                                                                            \
@@ -362,10 +377,8 @@ static int launch_ricci_group(const GridDims &g, const RfmArrays &rfm, const dou
 
 template <Variant V, typename T>
 static int launch_ricci_v(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
-  static_assert(kRicciGroups == 3, "group count");
-  BSSN_TRY((launch_ricci_group<V, 0, T>(g, rfm, in, aux, s)));
-  BSSN_TRY((launch_ricci_group<V, 1, T>(g, rfm, in, aux, s)));
-  return launch_ricci_group<V, 2, T>(g, rfm, in, aux, s);
+  return for_each_group<0, kRicciGroups>(
+      [&](auto gc) { return launch_ricci_group<V, decltype(gc)::value, T>(g, rfm, in, aux, s); });
 }
 
 int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s,
@@ -393,10 +406,8 @@ static int launch_rhs_group(const GridDims &g, const RfmArrays &rfm, const PhysP
 template <Variant V, typename T>
 static int launch_rhs_v(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp, const double *aux,
                         const double *in, double *rhs, cudaStream_t s) {
-  static_assert(kRhsGroups == 3, "group count");
-  BSSN_TRY((launch_rhs_group<V, T, 0>(g, rfm, pp, aux, in, rhs, s)));
-  BSSN_TRY((launch_rhs_group<V, T, 1>(g, rfm, pp, aux, in, rhs, s)));
-  return launch_rhs_group<V, T, 2>(g, rfm, pp, aux, in, rhs, s);
+  return for_each_group<0, kRhsGroups>(
+      [&](auto gc) { return launch_rhs_group<V, T, decltype(gc)::value>(g, rfm, pp, aux, in, rhs, s); });
 }
 
 int launch_rhs(Variant v, bool mixed, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
@@ -448,10 +459,8 @@ static int launch_fused_group(const GridDims &g, const RfmArrays &rfm, const Phy
 template <Variant V, typename T, int STAGE>
 static int launch_fused_stage_groups(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp, const double *aux,
                                      const StageBuffers &b, double *krhs, double dt, cudaStream_t s) {
-  static_assert(kRhsGroups == 3, "group count");
-  BSSN_TRY((launch_fused_group<V, T, STAGE, 0>(g, rfm, pp, aux, b, krhs, dt, s)));
-  BSSN_TRY((launch_fused_group<V, T, STAGE, 1>(g, rfm, pp, aux, b, krhs, dt, s)));
-  return launch_fused_group<V, T, STAGE, 2>(g, rfm, pp, aux, b, krhs, dt, s);
+  return for_each_group<0, kRhsGroups>(
+      [&](auto gc) { return launch_fused_group<V, T, STAGE, decltype(gc)::value>(g, rfm, pp, aux, b, krhs, dt, s); });
 }
 
 template <Variant V, typename T>
@@ -604,9 +613,9 @@ static int launch_fused_batched_group(const EvoDesc *descs, const int *tile_evo,
 template <Variant V, int STAGE>
 static int launch_fused_batched_stage(const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks, int bx,
                                       int by, cudaStream_t s) {
-  BSSN_TRY((launch_fused_batched_group<V, STAGE, 0>(descs, tile_evo, ntiles, blocks, bx, by, s)));
-  BSSN_TRY((launch_fused_batched_group<V, STAGE, 1>(descs, tile_evo, ntiles, blocks, bx, by, s)));
-  return launch_fused_batched_group<V, STAGE, 2>(descs, tile_evo, ntiles, blocks, bx, by, s);
+  return for_each_group<0, kRhsGroups>([&](auto gc) {
+    return launch_fused_batched_group<V, STAGE, decltype(gc)::value>(descs, tile_evo, ntiles, blocks, bx, by, s);
+  });
 }
 
 static int check_shape(int bx, int by) {
@@ -626,13 +635,13 @@ int launch_ricci_batched(Variant v, int stage, const EvoDesc *descs, const int *
     return BSSN_B200_EINVAL;
   }
   if (v == SPH_3D) {
-    BSSN_TRY((launch_ricci_batched_group<SPH_3D, 0>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
-    BSSN_TRY((launch_ricci_batched_group<SPH_3D, 1>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
-    return launch_ricci_batched_group<SPH_3D, 2>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+    return for_each_group<0, kRicciGroups>([&](auto gc) {
+      return launch_ricci_batched_group<SPH_3D, decltype(gc)::value>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+    });
   }
-  BSSN_TRY((launch_ricci_batched_group<SINH_3D, 0>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
-  BSSN_TRY((launch_ricci_batched_group<SINH_3D, 1>(stage, descs, tile_evo, ntiles, blocks, bx, by, s)));
-  return launch_ricci_batched_group<SINH_3D, 2>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+  return for_each_group<0, kRicciGroups>([&](auto gc) {
+    return launch_ricci_batched_group<SINH_3D, decltype(gc)::value>(stage, descs, tile_evo, ntiles, blocks, bx, by, s);
+  });
 }
 
 template <Variant V>
