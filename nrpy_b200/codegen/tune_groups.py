@@ -1,0 +1,234 @@
+"""Time candidate output groups and value allocations of the point kernels on a GPU.
+
+Code-generation-time tuning tool (the output-group split and the per-group allocation
+flags in generate.py come from its measurements). Three steps:
+
+  python -m nrpy_b200.codegen.tune_groups generate   # needs nrpy (equation modules)
+  python -m nrpy_b200.codegen.tune_groups compile    # nvcc, sm_100a, no GPU needed
+  python -m nrpy_b200.codegen.tune_groups run        # on a B200; prints one line per kernel
+
+`generate` emits every candidate group (Ricci: 1x6, 2x3, 3x2 (two pairings), 6x1 outputs;
+RHS: gauge/metric/extrinsic-curvature outputs merged or split in two or three parts) of the
+SinhSpherical 3-D algebra under three allocations (remat_first, deriv_remat) = (1,1),
+(1,0), (0,0) at a 90-value register budget, plus lower budgets with forced occupancy for
+the present groups. `compile` builds one timing executable per group into
+nrpy_b200/_tune/. `run` times each kernel alone on a 256x64x32 interior grid (+3 ghosts)
+of seeded values (median of 5 launches, CUDA events) and reports registers, local
+memory, slots and resident warps.
+"""
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import pathlib
+import subprocess
+import sys
+
+ROOT = pathlib.Path(__file__).resolve().parents[2]
+OUT = ROOT / "nrpy_b200" / "_tune"
+
+R = ["RbarDD00", "RbarDD01", "RbarDD02", "RbarDD11", "RbarDD12", "RbarDD22"]
+A = ["aDD00", "aDD01", "aDD02", "aDD11", "aDD12", "aDD22"]
+G1 = ["alpha", "cf", "hDD00", "hDD01", "hDD02", "hDD11", "hDD12", "hDD22", "trK", "vetU0", "vetU1", "vetU2"]
+G2 = ["betU0", "betU1", "betU2", "lambdaU0", "lambdaU1", "lambdaU2"]
+CANDIDATES = {
+    "ricci_1x6": ("ricci", R),
+    "ricci_012": ("ricci", R[:3]), "ricci_345": ("ricci", R[3:]),
+    "ricci_0001": ("ricci", R[0:2]), "ricci_0211": ("ricci", R[2:4]), "ricci_1222": ("ricci", R[4:6]),
+    "ricci_0011": ("ricci", [R[0], R[3]]), "ricci_0112": ("ricci", [R[1], R[4]]), "ricci_0222": ("ricci", [R[2], R[5]]),
+    **{f"ricci_{k}": ("ricci", [k]) for k in R},
+    "rhs_a": ("rhs", A), "rhs_a3a": ("rhs", A[:3]), "rhs_a3b": ("rhs", A[3:]),
+    "rhs_g1": ("rhs", G1), "rhs_g1_scalar_vet": ("rhs", ["alpha", "cf", "trK", "vetU0", "vetU1", "vetU2"]),
+    "rhs_g1_h": ("rhs", G1[2:8]), "rhs_g1_scalar": ("rhs", ["alpha", "cf", "trK"]), "rhs_vet": ("rhs", G1[9:]),
+    "rhs_a_g1": ("rhs", A + G1), "rhs_a_scalar": ("rhs", A + ["alpha", "cf", "trK"]),
+    "rhs_h_vet": ("rhs", G1[2:8] + G1[9:]),
+    "rhs_g2": ("rhs", G2), "rhs_lambda": ("rhs", G2[3:]), "rhs_bet": ("rhs", G2[:3]),
+}
+ALLOCS = [(90, True, True, 1), (90, True, False, 1), (90, False, False, 1)]
+# lower register budgets with forced occupancy (launch_bounds min blocks per SM of 128 threads)
+LOW = [(60, True, True, 3), (48, True, True, 4)]
+LOW_GROUPS = {"ricci_0001", "ricci_0211", "ricci_1222", "rhs_a", "rhs_g1", "rhs_g2"}
+
+HARNESS_HEAD = r'''
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include <cuda_runtime.h>
+struct RfmArrays { const double *f0, *f0_D0, *f0_DD00, *f0_DDD000, *f1, *f1_D1, *f1_DD11; };
+template <typename T> __device__ __forceinline__ T ipow(T x, int n) { T r = x; for (int k = 1; k < n; k++) r *= x; return r; }
+struct PointCtx {
+  const double *__restrict__ in; const double *__restrict__ aux; int s1, s2, ntot; int i0, i1;
+  double invdxx0, invdxx1, invdxx2; RfmArrays rfm; double eta, KreissOliger_strength_gauge, KreissOliger_strength_nongauge;
+  __device__ __forceinline__ double ld(int gf, int a, int b, int c) const { return __ldg(in + (gf * ntot + (a + b * s1 + c * s2))); }
+  __device__ __forceinline__ double ldaux(int k) const { return __ldg(aux + k * ntot); }
+};
+#define LD(gf, a, b, c) ctx.ld(gf, a, b, c)
+#define LDAUX(k) ctx.ldaux(k)
+#define RFM(arr, d) __ldg(ctx.rfm.arr + ctx.i##d)
+#define rfm_f0 f0
+#define rfm_f0_D0 f0_D0
+#define rfm_f0_DD00 f0_DD00
+#define rfm_f0_DDD000 f0_DDD000
+#define rfm_f1 f1
+#define rfm_f1_D1 f1_D1
+#define rfm_f1_DD11 f1_DD11
+#define PARAM(name) ctx.name
+#define SMEM(k) sm[(k) * NT]
+#define invdxx0 ctx.invdxx0
+#define invdxx1 ctx.invdxx1
+#define invdxx2 ctx.invdxx2
+#include "GROUP.cuh"
+#undef invdxx0
+#undef invdxx1
+#undef invdxx2
+constexpr int N0 = 262, N1 = 70, N2 = 38, NTOT = N0 * N1 * N2, MAXOUT = 18;
+template <int NT, int MINB, int NOUT, class F>
+__global__ void __launch_bounds__(NT, MINB) kern(RfmArrays rfm, const double *in, const double *aux, double *out) {
+  const int i0 = 3 + blockIdx.x * 32 + threadIdx.x, i1 = 3 + blockIdx.y * (NT / 32) + threadIdx.y, i2 = 3 + blockIdx.z;
+  if (i0 >= N0 - 3 || i1 >= N1 - 3) return;
+  extern __shared__ double smem[];
+  volatile double *sm = smem + threadIdx.x + 32 * threadIdx.y;
+  const int idx = i0 + N0 * i1 + N0 * N1 * i2;
+  PointCtx ctx;
+  ctx.in = in + idx; ctx.aux = aux + idx; ctx.s1 = N0; ctx.s2 = N0 * N1; ctx.ntot = NTOT; ctx.i0 = i0; ctx.i1 = i1;
+  ctx.invdxx0 = 10.0; ctx.invdxx1 = 20.0; ctx.invdxx2 = 5.0; ctx.rfm = rfm; ctx.eta = 1.0;
+  ctx.KreissOliger_strength_gauge = 0.3; ctx.KreissOliger_strength_nongauge = 0.3;
+  double o[NOUT];
+  F::template eval<NT>(ctx, o, sm);
+#pragma unroll
+  for (int k = 0; k < NOUT; k++) out[idx + k * NTOT] = o[k];
+}
+template <int NT, int MINB, int NOUT, int SLOTS, class F>
+void run(const char *name, RfmArrays rfm, const double *in, const double *aux, double *out) {
+  auto K = kern<NT, MINB, NOUT, F>;
+  const size_t sb = (size_t)SLOTS * NT * 8;
+  if (sb > 227 * 1024) { printf("{\"kernel\": \"%s\", \"skip\": \"shared memory\"}\n", name); return; }
+  if (cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb) != cudaSuccess) return;
+  cudaFuncAttributes at;
+  cudaFuncGetAttributes(&at, K);
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, K, NT, sb);
+  const dim3 grid(8, 64 / (NT / 32), 32);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  for (int w = 0; w < 2; w++) K<<<grid, dim3(32, NT / 32), sb>>>(rfm, in, aux, out);
+  std::vector<float> ts;
+  for (int r = 0; r < 5; r++) {
+    cudaEventRecord(a);
+    K<<<grid, dim3(32, NT / 32), sb>>>(rfm, in, aux, out);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms;
+    cudaEventElapsedTime(&ms, a, b);
+    ts.push_back(ms);
+  }
+  std::sort(ts.begin(), ts.end());
+  const cudaError_t e = cudaGetLastError();
+  printf("{\"kernel\": \"%s\", \"threads\": %d, \"min_blocks\": %d, \"regs\": %d, \"local_bytes\": %zu, \"slots\": %d, "
+         "\"warps_per_sm\": %d, \"us\": %.1f, \"error\": \"%s\"}\n", name, NT, MINB, at.numRegs, at.localSizeBytes, SLOTS,
+         nb * NT / 32, ts[2] * 1e3, e == cudaSuccess ? "" : cudaGetErrorString(e));
+}
+int main() {
+  std::vector<double> h((size_t)NTOT * 24);
+  srand(7);
+  for (auto &x : h) x = 0.5 + (double)rand() / RAND_MAX;
+  double *in, *aux, *out, *r[7];
+  cudaMalloc(&in, h.size() * 8);
+  cudaMemcpy(in, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
+  cudaMalloc(&aux, (size_t)NTOT * 6 * 8);
+  cudaMemcpy(aux, h.data(), (size_t)NTOT * 6 * 8, cudaMemcpyHostToDevice);
+  cudaMalloc(&out, (size_t)NTOT * MAXOUT * 8);
+  for (int k = 0; k < 7; k++) {
+    cudaMalloc(&r[k], 300 * 8);
+    cudaMemcpy(r[k], h.data() + 1000 * k, 300 * 8, cudaMemcpyHostToDevice);
+  }
+  RfmArrays rfm{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
+'''
+
+
+def generate() -> None:
+    from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen.emit_cuda import emit_point_function
+
+    be.setup_nrpy("")
+    rhs, betaU = be.rhs_exprs("SinhSpherical")
+    ricci = be.ricci_exprs("SinhSpherical")
+    OUT.mkdir(parents=True, exist_ok=True)
+    for gname, (kind, names) in CANDIDATES.items():
+        src, uv = (ricci, None) if kind == "ricci" else (rhs, betaU)
+        allocs = ALLOCS + (LOW if gname in LOW_GROUPS else [])
+        parts, wrappers, calls = ["#pragma once\n"], [], []
+        for cap, rf, dr, minb in allocs:
+            fname = f"{gname}_c{cap}_r{int(rf)}_d{int(dr)}"
+            code, st = emit_point_function(fname, [(f"out[{i}]", src[n]) for i, n in enumerate(names)],
+                                           upwind_vec=uv, reg_capacity=cap, remat_first=rf, deriv_remat=dr)
+            parts.append(code)
+            slots = max(st["smem_slots"], 1)
+            wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
+                            f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
+            nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
+            launches = [(nt, minb)] if minb == 1 else [(128, minb), (64, 2 * minb)]
+            if minb == 1 and nt == 128:
+                launches.append((64, 1))
+            for t, mb in launches:
+                calls.append(f'  run<{t}, {mb}, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+        (OUT / f"{gname}.cuh").write_text("\n".join(parts))
+        head, main = HARNESS_HEAD.replace("GROUP", gname).split("int main() {")
+        body = head + "\n".join(wrappers) + "\nint main() {" + main
+        (OUT / f"{gname}.cu").write_text(body + "\n".join(calls) + "\n  return 0;\n}\n")
+        print(gname, flush=True)
+
+
+def compile_all(jobs: int) -> None:
+    from nrpy_b200.build import nvcc
+
+    cc = nvcc()
+
+    def one(cu: pathlib.Path) -> str:
+        exe = cu.with_suffix("")
+        r = subprocess.run([cc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
+                            "--expt-relaxed-constexpr", "-o", str(exe), str(cu)], capture_output=True, text=True)
+        return f"{cu.name}: {'ok' if r.returncode == 0 else 'FAILED ' + r.stderr[-500:]}"
+
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        for line in ex.map(one, sorted(OUT.glob("*.cu"))):
+            print(line, flush=True)
+
+
+def run_all() -> None:
+    for exe in sorted(p for p in OUT.iterdir() if p.is_file() and p.suffix == "" and os.access(p, os.X_OK)):
+        r = subprocess.run([str(exe)], capture_output=True, text=True)
+        sys.stdout.write(r.stdout)
+        if r.returncode != 0:
+            raise SystemExit(f"{exe.name} exited {r.returncode}: {r.stderr[-500:]}")
+
+
+def summarize(path: str) -> None:
+    rows = [json.loads(ln) for ln in open(path) if ln.startswith("{") and "us" in ln]
+    best = {}
+    for r in rows:
+        g = r["kernel"].rsplit("_c", 1)[0]
+        if g not in best or r["us"] < best[g]["us"]:
+            best[g] = r
+    for g, r in sorted(best.items()):
+        print(f"{g:22s} {r['us']:8.1f} us  {r['kernel']}  threads={r['threads']} regs={r['regs']} "
+              f"local={r['local_bytes']} slots={r['slots']} warps/SM={r['warps_per_sm']}")
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("step", choices=["generate", "compile", "run", "summarize"])
+    ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
+    ap.add_argument("--log", default=None)
+    a = ap.parse_args()
+    if a.step == "generate":
+        generate()
+    elif a.step == "compile":
+        compile_all(a.jobs)
+    elif a.step == "run":
+        run_all()
+    else:
+        summarize(a.log)
