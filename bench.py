@@ -194,6 +194,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-diff", action="store_true", help="skip the adjoint-gradient section")
+    ap.add_argument("--diff-only", action="store_true",
+                    help="run only the adjoint-gradient section (one GPU) and print it as JSON (profiling)")
     ap.add_argument("--nxx", default=None, help="override the grid, e.g. 256,64,32 (profiling only)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -202,6 +204,9 @@ def main():
         NXX = tuple(int(x) for x in args.nxx.split(","))
     if args.impl == "reference":
         return run_reference(args)
+    if args.diff_only:
+        print(json.dumps(run_differentiation(fd_check=False)))
+        return None
 
     import torch
 

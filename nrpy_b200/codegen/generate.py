@@ -63,7 +63,12 @@ def threads_for(slots: int) -> int:
 # Reverse-mode (adjoint) functions: generated for these variants only; fewer values in
 # registers because the VJP kernels run 64 threads per block with shared-memory slots.
 ADJOINT_VARIANTS = ["sph_3d"]
+# VJP kernels run 64 threads per block; recompute-first eviction and rematerialized finite
+# differences shrink the slot arrays of the largest group from 250 to 199 values (2 blocks
+# per SM instead of 1): the 200-step backward of the 128x32x32 workload went from 3.42 s to
+# 2.84 s on a B200 (a 90-value budget gave 2.84 s with more spills).
 ADJ_REG_CAPACITY = 64
+ADJ_REMAT = dict(remat_first=True, deriv_remat=True)
 
 
 def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int) -> str:
@@ -237,7 +242,7 @@ def generate_adjoint(tag: str) -> None:
         fname = f"ricci_vjp_{tag}_g{g}"
         code, st = emit_vjp_function(fname, [ricci[k] for k in gnames], row_of, symmetry_axes=sym,
                                      comment=f"VJP of Rbar_ij {gnames} (Ricci_eval.py:27-167)",
-                                     reg_capacity=ADJ_REG_CAPACITY)
+                                     reg_capacity=ADJ_REG_CAPACITY, **ADJ_REMAT)
         parts.append(code)
         stats[f"ricci_g{g}"] = st
         structs.append(_vjp_struct("RicciVjp", tag, g, fname, [be.RBAR_ORDER.index(k) for k in gnames],
@@ -246,21 +251,21 @@ def generate_adjoint(tag: str) -> None:
         fname = f"rhs_vjp_{tag}_g{g}"
         code, st = emit_vjp_function(fname, [rhs[k] for k in gnames], row_of, upwind_vec=betaU,
                                      symmetry_axes=sym, comment=f"VJP of the RHS of {gnames} (rhs_eval.py:122-220)",
-                                     reg_capacity=ADJ_REG_CAPACITY)
+                                     reg_capacity=ADJ_REG_CAPACITY, **ADJ_REMAT)
         parts.append(code)
         stats[f"rhs_g{g}"] = st
         structs.append(_vjp_struct("RhsVjp", tag, g, fname, [be.GF_ORDER.index(k) for k in gnames],
                                    st["smem_slots"]))
     code, st = emit_vjp_function(f"h_vjp_{tag}", [cons["H"]], row_of, symmetry_axes=sym,
                                  comment="VJP of the Hamiltonian constraint H (constraints_eval.py:364-492)",
-                                 reg_capacity=ADJ_REG_CAPACITY)
+                                 reg_capacity=ADJ_REG_CAPACITY, **ADJ_REMAT)
     parts.append(code)
     stats["H"] = st
     hnames = ["hDD00", "hDD01", "hDD02", "hDD11", "hDD12", "hDD22"]
     code, st = emit_vjp_function(f"enforce_vjp_{tag}", [enf[k] for k in hnames], row_of, symmetry_axes=sym,
                                  comment="VJP of the detgammabar projection "
                                  "(enforce_detgammabar_equals_detgammahat.py:85-110)",
-                                 reg_capacity=ADJ_REG_CAPACITY)
+                                 reg_capacity=ADJ_REG_CAPACITY, **ADJ_REMAT)
     parts.append(code)
     stats["enforce"] = st
     pk = PointKernel(sym)

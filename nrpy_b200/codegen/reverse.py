@@ -111,7 +111,8 @@ def leaf_table(names: Sequence[str]) -> List[Tuple[str, int, int, int, int]]:
 
 
 def emit_vjp_function(fname: str, outputs: Sequence[sp.Expr], row_of: Dict[str, int], upwind_vec=None,
-                      symmetry_axes: str = "", comment: str = "", reg_capacity: int = 64):
+                      symmetry_axes: str = "", comment: str = "", reg_capacity: int = 64, remat_first: bool = False,
+                      deriv_remat: bool = False):
     """Emit the VJP of `outputs` as `fname(ctx, sm)` plus `fname_SMEM_SLOTS`.
 
     Gridfunction and derivative leaf adjoints go to OUT(row_of[name]); Rbar_ij adjoints
@@ -123,7 +124,7 @@ def emit_vjp_function(fname: str, outputs: Sequence[sp.Expr], row_of: Dict[str, 
         lhs = f"OUTR({RBAR_INDEX[name]})" if name in RBAR_INDEX else f"OUT({row_of[name]})"
         outs.append((lhs, leaf_adj[name]))
     pk.build_program(stmts, outs, upwind_vec)
-    lines, nslots = allocate_values(dfs_order(pk.lines), reg_capacity)
+    lines, nslots = allocate_values(dfs_order(pk.lines), reg_capacity, remat_first, deriv_remat)
     body = "\n".join("  " + ln for ln in lines)
     head = f"// {comment}\n" if comment else ""
     code = (
