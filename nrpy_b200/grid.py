@@ -225,6 +225,56 @@ class BSSNGrid:
         for _ in range(nsteps):
             L.check(self.lib.bssn_b200_mol_step(C.byref(self.cd), self.gd, mode, int(mixed), self.stream))
 
+    def step_from_host(self, host_in: Sequence[torch.Tensor], host_out: Sequence[torch.Tensor], mode: int = 1,
+                       mixed: bool = False, on_step=None) -> None:
+        """One RK4 step for each host state: host_in[i] (pinned, NUM_EVOL_GFS gridfunctions)
+        -> device -> one step -> host_out[i].
+
+        The copies overlap the steps: the state alternates between two device buffers, the
+        upload of state i+1 runs on its own stream during step i and the download of state i
+        on a third stream during step i+1. Steps run in order on the current stream (they share
+        the grid's stage buffers). ``on_step(i, y)`` (optional) is called on the current stream
+        after step i with the device state. y_n_gfs points at this grid's own y_n again on return."""
+        n = len(host_in)
+        if len(host_out) != n:
+            raise ValueError("host_in and host_out must have the same length")
+        if getattr(self, "_y_alt", None) is None:
+            self._y_alt = torch.empty_like(self.y_n)
+        dev = [self.y_n, self._y_alt]
+        comp = torch.cuda.current_stream(self.device)
+        h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
+        h2d.wait_stream(comp)
+        d2h.wait_stream(comp)
+        freed = [None, None]  # event: the last download from buffer k has finished
+        gf = self.gd[0].gridfuncs
+        try:
+            for i in range(n):
+                k = i % 2
+                with torch.cuda.stream(h2d):
+                    if freed[k] is not None:
+                        h2d.wait_event(freed[k])
+                    dev[k].copy_(host_in[i], non_blocking=True)
+                    loaded = torch.cuda.Event()
+                    loaded.record(h2d)
+                comp.wait_event(loaded)
+                gf.y_n_gfs = _ptr(dev[k])
+                L.check(self.lib.bssn_b200_mol_step(C.byref(self.cd), self.gd, mode, int(mixed),
+                                                    C.c_void_p(comp.cuda_stream)))
+                if on_step is not None:
+                    on_step(i, dev[k])
+                stepped = torch.cuda.Event()
+                stepped.record(comp)
+                with torch.cuda.stream(d2h):
+                    d2h.wait_event(stepped)
+                    host_out[i].copy_(dev[k], non_blocking=True)
+                    done = torch.cuda.Event()
+                    done.record(d2h)
+                freed[k] = done
+        finally:
+            gf.y_n_gfs = _ptr(self.y_n)
+            comp.wait_stream(h2d)
+            comp.wait_stream(d2h)
+
     def make_stepper(self, mode: int = 1, mixed: bool = False, steps_per_graph: int = 1, stream=None):
         """Capture `steps_per_graph` RK4 steps into a CUDA graph bound to this grid's buffers."""
         self.free_stepper()
