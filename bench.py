@@ -194,6 +194,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-diff", action="store_true", help="skip the adjoint-gradient section")
+    ap.add_argument("--no-diag", action="store_true", help="skip the diagnostics-output section")
     ap.add_argument("--diff-only", action="store_true",
                     help="run only the adjoint-gradient section (one GPU) and print it as JSON (profiling)")
     ap.add_argument("--nxx", default=None, help="override the grid, e.g. 256,64,32 (profiling only)")
@@ -275,6 +276,7 @@ def main():
 
     # ---------------- end-to-end through the public API with host buffers
     e2e = None if args.no_e2e else run_e2e(grid, args, y0)
+    diag = None if (args.no_diag or rank != 0) else run_diagnostics(grid, args)
     grid_dt = grid.dt
     grid.free_stepper()
     grid.close()
@@ -316,6 +318,7 @@ def main():
             "mixed": mixed,
             "batched": batched,
             "differentiation": differentiation,
+            "diagnostics": diag,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -416,6 +419,57 @@ def run_batched(args, world, rank, dist):
             "interior_points": pts if dist is None else None, "tile": list(tune["tile"]), "blocks": tune["blocks"],
             "autotune": tune["table"], "graph_kernel_nodes_per_replay": info["kernel_nodes"],
             "sequential_single_grid_value": seq_value, "speedup_vs_sequential": value / seq_value}
+
+
+def run_diagnostics(grid, args, reps: int = 3):
+    """One diagnostics() output step of the bench grid (Ricci + constraints on the device,
+    nearest-point samples gathered on the device, volume integrals reduced on the device,
+    the reference's ASCII files written), wall time per output step; beside it the
+    reference's own diagnostics() on the host cores on the same grid and state."""
+    import torch
+
+    cwd = os.getcwd()
+    res = {}
+    with tempfile.TemporaryDirectory() as d:
+        os.chdir(d)
+        try:
+            grid.diagnostics(1.0, nn=0, time=0.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for k in range(reps):
+                grid.diagnostics(1.0, nn=k + 1, time=0.0)
+            torch.cuda.synchronize()
+            res["ms_per_output"] = 1e3 * (time.perf_counter() - t0) / reps
+            res["files"] = sorted(os.listdir(d))
+        finally:
+            os.chdir(cwd)
+    n1, n2 = grid.N[1] - 6, grid.N[2] - 6
+    n0 = grid.N[0] - 6
+    samples = 1 + 4 * n0 + n0 * n2 + 2 * n0 * n1
+    res["d2h_bytes_per_output"] = samples * 2 * 8 + 8 * 8
+    res["reference_cuda_path_d2h_bytes_per_output"] = grid.y_n.numel() * 8
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+
+            if ref.available("sinh3d"):
+                m1, z1, m2, z2 = bl_params(args.seed)
+                rg = ref.RefGrid("sinh3d", NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2,
+                                 BH2_posn_z=z2)
+                with tempfile.TemporaryDirectory() as d:
+                    os.chdir(d)
+                    try:
+                        rg.diagnostics(0, 0.0, 1.0)
+                        t0 = time.perf_counter()
+                        rg.diagnostics(1, 0.0, 1.0)
+                        res["reference_ms_per_output"] = 1e3 * (time.perf_counter() - t0)
+                    finally:
+                        os.chdir(cwd)
+                rg.close()
+                res["reference_cores"] = os.cpu_count()
+        except Exception as e:  # noqa: BLE001
+            res["reference_unavailable"] = str(e)
+    return res
 
 
 def run_differentiation(fd_check: bool = True):

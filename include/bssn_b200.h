@@ -49,6 +49,16 @@ enum {
 enum { RBARDD00GF, RBARDD01GF, RBARDD02GF, RBARDD11GF, RBARDD12GF, RBARDD22GF };
 /* Diagnostic gridfunctions written by constraints_eval() (a 3-slot array). */
 enum { BSSN_B200_DIAG_HAMILTONIAN, BSSN_B200_DIAG_MSQUARED, BSSN_B200_DIAG_LAMBDA_CONSTRAINT, BSSN_B200_NUM_DIAG_GFS };
+/* The generated project's diagnostic gridfunctions (its diagnostics/diagnostic_gfs.h, the
+ * DIAG_* enum of two_blackholes_collide): the layout of the diagnostic_gfs arrays that the
+ * drop-ins constraints_eval, diagnostic_gfs_set, diagnostics_nearest and
+ * diagnostics_volume_integration read and write. */
+enum {
+  BSSN_B200_DIAG_GRIDINDEXGF, BSSN_B200_DIAG_HAMILTONIANGF, BSSN_B200_DIAG_LAMBDA_CONSTRAINTGF, BSSN_B200_DIAG_LAPSEGF,
+  BSSN_B200_DIAG_MSQUAREDGF, BSSN_B200_DIAG_RBARDD00GF, BSSN_B200_DIAG_RBARDD01GF, BSSN_B200_DIAG_RBARDD02GF,
+  BSSN_B200_DIAG_RBARDD11GF, BSSN_B200_DIAG_RBARDD12GF, BSSN_B200_DIAG_RBARDD22GF, BSSN_B200_DIAG_WGF,
+  BSSN_B200_TOTAL_NUM_DIAG_GFS
+};
 
 /* CoordSystem_hash values (BHaH_defines.h). */
 #define SPHERICAL 1307621703
@@ -233,10 +243,35 @@ void enforce_detgammabar_equals_detgammahat(const params_struct *params, const r
                                             const REAL *auxevol_gfs);
 /* MoLtimestepping/MoL_step_forward_in_time.py:39-507 (RK4, radiation or extrapolation outer BCs). */
 void MoL_step_forward_in_time(commondata_struct *commondata, griddata_struct *griddata);
-/* general_relativity/constraints_eval.py:364-492 -- diagnostic_gfs holds BSSN_B200_NUM_DIAG_GFS gridfunctions
- * (H, M^2, |Lambda constraint|) on the device; interior points are written. */
+/* general_relativity/constraints_eval.py:364-492 -- diagnostic_gfs holds BSSN_B200_TOTAL_NUM_DIAG_GFS
+ * gridfunctions on the device (the generated project's layout); H, M^2 and |Lambda constraint| are written at
+ * the interior points of BSSN_B200_DIAG_HAMILTONIANGF, _MSQUAREDGF and _LAMBDA_CONSTRAINTGF. */
 void constraints_eval(const commondata_struct *commondata, const params_struct *params, const rfm_struct *rfmstruct,
                       const REAL *in_gfs, const REAL *auxevol_gfs, REAL *diagnostic_gfs);
+
+/* ---- diagnostics (diagnostics/diagnostics.py:46-270 and the helpers it registers) ----
+ * Diagnostic arrays are DEVICE arrays of BSSN_B200_TOTAL_NUM_DIAG_GFS gridfunctions; samples are
+ * gathered on the GPU and only they are copied to the host. Output files (the reference's names and
+ * ASCII formats) go to the current directory:
+ *   out0d-grid%02d-<Coord>-conv_factor-%.2f.txt            H, M^2 at the point next to the origin
+ *   out1d-{y,z}-<Coord>-grid%02d-conv_factor%.2f-t%08.2f.txt  H, M^2 along the lines nearest the y, z axes
+ *   out2d-{xy,yz}-<Coord>-grid%02d-conv_factor%.2f-t%08.2f.txt H, M^2 on the planes nearest xy, yz
+ *   out3d-integrals-conv_factor%.2f-<recipe>.txt            volume integrals, L2 and RMS of H, M^2, |Lambda|
+ *     over recipes "whole_domain" and "sphere_R_gt_8" (r > 8), as two_blackholes_collide defines them. */
+/* diagnostics.py:46-270 -- on output steps (|round(t/every)*every - t| < dt/2): diagnostic_gfs_set,
+ * diagnostics_nearest, diagnostics_volume_integration; then progress_indicator. */
+void diagnostics(commondata_struct *commondata, griddata_struct *griddata);
+/* diagnostic_gfs_set: Ricci, constraints, lapse, W, grid index (and Rbar_ij) into each grid's array. */
+void diagnostic_gfs_set(const commondata_struct *commondata, const griddata_struct *griddata,
+                        REAL *diagnostic_gfs[MAXNUMGRIDS]);
+/* diagnostics_nearest.c / diagnostics_nearest_{grid_center,1d_y_and_z_axes,2d_xy_and_yz_planes}. */
+void diagnostics_nearest(commondata_struct *commondata, griddata_struct *griddata,
+                         const REAL *diagnostic_gfs[MAXNUMGRIDS]);
+/* diagnostics_volume_integration.c + diagnostics_volume_integration_helpers.h. */
+void diagnostics_volume_integration(commondata_struct *commondata, griddata_struct *griddata,
+                                    const REAL *diagnostic_gfs[MAXNUMGRIDS]);
+/* progress_indicator.py: one status line on stderr every output_progress_every steps. */
+void progress_indicator(commondata_struct *commondata, const griddata_struct *griddata);
 
 /* ======================= status-returning entry points (explicit stream) ======================= */
 /* `stream` is a cudaStream_t passed as void* (NULL = legacy default stream). Return 0 on success,
@@ -272,6 +307,7 @@ int bssn_b200_apply_bcs_inner_only(const params_struct *params, const bc_struct 
                                    const int8_t *gf_parity_types, void *stream);
 int bssn_b200_enforce_detgammabar_equals_detgammahat(const params_struct *params, const rfm_struct *rfmstruct,
                                                      REAL *in_gfs, void *stream);
+/* Compact layout: diagnostic_gfs holds BSSN_B200_NUM_DIAG_GFS gridfunctions (H, M^2, |Lambda|). */
 int bssn_b200_constraints_eval(const commondata_struct *commondata, const params_struct *params,
                                const rfm_struct *rfmstruct, const REAL *in_gfs, const REAL *auxevol_gfs,
                                REAL *diagnostic_gfs, void *stream);
@@ -355,6 +391,10 @@ int bssn_b200_adjoint_functional_vjp(bssn_b200_adjoint *adj, const double *y, do
 int bssn_b200_adjoint_step_vjp(bssn_b200_adjoint *adj, const double *y_n, double *ybar);
 int bssn_b200_adjoint_id_vjp(bssn_b200_adjoint *adj, const double *ybar0, double grad[4]);
 int bssn_b200_adjoint_destroy(bssn_b200_adjoint *adj);
+
+/* The diagnostics() driver with a status return and an explicit stream (the diagnostic arrays are
+ * kept by the library per grid and reused). */
+int bssn_b200_diagnostics(commondata_struct *commondata, griddata_struct *griddata, void *stream);
 
 /* Instrumentation: kernels launched by this library since it was loaded (each graph replay
  * counts its kernel nodes), and a launch of only the interior RHS + RK-update + projection

@@ -458,8 +458,20 @@ void MoL_step_forward_in_time(commondata_struct *commondata, griddata_struct *gr
 }
 void constraints_eval(const commondata_struct *commondata, const params_struct *params, const rfm_struct *rfmstruct,
                       const REAL *in_gfs, const REAL *auxevol_gfs, REAL *diagnostic_gfs) {
-  die_on(bssn_b200_constraints_eval(commondata, params, rfmstruct, in_gfs, auxevol_gfs, diagnostic_gfs, nullptr),
-         __func__);
+  // The generated project's diagnostic array: BSSN_B200_TOTAL_NUM_DIAG_GFS gridfunctions.
+  (void)commondata;
+  static const int slots[3] = {BSSN_B200_DIAG_HAMILTONIANGF, BSSN_B200_DIAG_MSQUAREDGF,
+                               BSSN_B200_DIAG_LAMBDA_CONSTRAINTGF};
+  int rc = check_ptr(rfmstruct, "rfmstruct");
+  if (rc == BSSN_B200_OK) rc = check_ptr(in_gfs, "in_gfs");
+  if (rc == BSSN_B200_OK) rc = check_ptr(auxevol_gfs, "auxevol_gfs");
+  if (rc == BSSN_B200_OK) rc = check_ptr(diagnostic_gfs, "diagnostic_gfs");
+  Variant v;
+  if (rc == BSSN_B200_OK) rc = variant_of(params, &v);
+  if (rc == BSSN_B200_OK)
+    rc = launch_constraints(v, grid_dims(params), rfm_arrays(rfmstruct), in_gfs, auxevol_gfs, diagnostic_gfs, nullptr,
+                            slots);
+  die_on(rc, __func__);
 }
 
 }  // extern "C"

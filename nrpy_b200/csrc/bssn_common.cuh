@@ -87,8 +87,9 @@ int launch_ricci(Variant v, const GridDims &g, const RfmArrays &rfm, const doubl
                  bool mixed = false);
 int launch_rhs(Variant v, bool mixed, const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
                const double *aux, const double *in, double *rhs, cudaStream_t s);
+// H, M^2, |Lambda| at interior points into diag gridfunctions slots[0..2] (default 0, 1, 2).
 int launch_constraints(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, const double *aux,
-                       double *diag, cudaStream_t s);
+                       double *diag, cudaStream_t s, const int *slots = nullptr);
 int launch_enforce(Variant v, const GridDims &g, const RfmArrays &rfm, double *gfs, cudaStream_t s);
 int launch_lambda_id(Variant v, const GridDims &g, const RfmArrays &rfm, double *gfs, cudaStream_t s);
 

@@ -188,14 +188,15 @@ template <Variant V>
 __global__ void __launch_bounds__(BX *BY, 1) constraints_kernel(const GridDims g, const RfmArrays rfm,
                                                              const double *__restrict__ in,
                                                              const double *__restrict__ aux,
-                                                             double *__restrict__ diag) {
+                                                             double *__restrict__ diag, const int3 slot) {
   INTERIOR_INDEX_OR_RETURN(g);
   const PointCtx ctx = make_ctx(g, rfm, in, aux, i0, i1, i2);
   double out[3];
   DISPATCH_POINT(constraints_point, V, double, double, ctx, out);
-  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
-#pragma unroll
-  for (int k = 0; k < 3; k++) diag[idx + k * g.ntot] = out[k];
+  const size_t idx = (size_t)i0 + (size_t)g.s1 * i1 + (size_t)g.s2 * i2;
+  diag[idx + (size_t)slot.x * g.ntot] = out[0];
+  diag[idx + (size_t)slot.y * g.ntot] = out[1];
+  diag[idx + (size_t)slot.z * g.ntot] = out[2];
 }
 
 // lambda^i = Lambdabar^i / ReU[i] from centred derivatives of hDD (initial data;
@@ -422,9 +423,10 @@ int launch_rhs(Variant v, bool mixed, const GridDims &g, const RfmArrays &rfm, c
 }
 
 int launch_constraints(Variant v, const GridDims &g, const RfmArrays &rfm, const double *in, const double *aux,
-                       double *diag, cudaStream_t s) {
+                       double *diag, cudaStream_t s, const int *slots) {
   if (empty_interior(g)) return BSSN_B200_OK;
-  VARIANT_SWITCH(v, (constraints_kernel<VV><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, in, aux, diag)));
+  const int3 sl = slots ? make_int3(slots[0], slots[1], slots[2]) : make_int3(0, 1, 2);
+  VARIANT_SWITCH(v, (constraints_kernel<VV><<<interior_grid(g), dim3(BX, BY), 0, s>>>(g, rfm, in, aux, diag, sl)));
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }

@@ -220,6 +220,18 @@ class BSSNGrid:
         res["volume"] = vol
         return res
 
+    def diagnostics(self, output_every: float, nn: Optional[int] = None, time: Optional[float] = None) -> None:
+        """The generated project's diagnostics() on this grid: on output steps (time within dt/2
+        of a multiple of output_every) the out0d/out1d/out2d/out3d-integrals files are written to
+        the current directory. nn and time default to the grid's step counter and time."""
+        cd = self.cd
+        if nn is not None:
+            cd.nn = int(nn)
+        if time is not None:
+            cd.time = float(time)
+        cd.diagnostics_output_every = float(output_every)
+        L.check(self.lib.bssn_b200_diagnostics(C.byref(cd), self.gd, self.stream))
+
     # ------------------------------------------------------------------ time stepping
     def MoL_step_forward_in_time(self, mode: int = 1, mixed: bool = False, nsteps: int = 1) -> None:
         for _ in range(nsteps):

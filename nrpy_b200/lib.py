@@ -13,6 +13,11 @@ NGHOSTS = 3
 NUM_EVOL_GFS = 24
 NUM_AUXEVOL_GFS = 6
 NUM_DIAG_GFS = 3
+# The generated project's diagnostic gridfunctions (BSSN_B200_DIAG_*GF of bssn_b200.h).
+DIAG_GFS = ["DIAG_GRIDINDEX", "DIAG_HAMILTONIAN", "DIAG_LAMBDA_CONSTRAINT", "DIAG_LAPSE", "DIAG_MSQUARED",
+            "DIAG_RBARDD00", "DIAG_RBARDD01", "DIAG_RBARDD02", "DIAG_RBARDD11", "DIAG_RBARDD12", "DIAG_RBARDD22",
+            "DIAG_W"]
+TOTAL_NUM_DIAG_GFS = len(DIAG_GFS)
 MAXNUMGRIDS = 15
 SPHERICAL = 1307621703
 SINHSPHERICAL = 579707936
@@ -150,6 +155,12 @@ SIGNATURES = [
     ("enforce_detgammabar_equals_detgammahat", None, [PP, PRFM, PR, PR]),
     ("MoL_step_forward_in_time", None, [PCD, PGD]),
     ("constraints_eval", None, [PCD, PP, PRFM, PR, PR, PR]),
+    ("diagnostics", None, [PCD, PGD]),
+    ("diagnostic_gfs_set", None, [PCD, PGD, C.POINTER(PR)]),
+    ("diagnostics_nearest", None, [PCD, PGD, C.POINTER(PR)]),
+    ("diagnostics_volume_integration", None, [PCD, PGD, C.POINTER(PR)]),
+    ("progress_indicator", None, [PCD, PGD]),
+    ("bssn_b200_diagnostics", C.c_int, [PCD, PGD, V]),
     ("bssn_b200_last_error", C.c_char_p, []),
     ("bssn_b200_version", C.c_char_p, []),
     ("bssn_b200_set_symmetry_axes", C.c_int, [C.c_char_p]),

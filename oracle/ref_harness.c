@@ -187,3 +187,11 @@ double ref_dV(ref_sim *s, int i0, int i1, int i2) {
   sqrt_detgammahat_d3xx_volume_element(&g->params, g->xx[0][i0], g->xx[1][i1], g->xx[2][i2], &dV);
   return dV;
 }
+// The generated project's diagnostics() driver at the present state: output cadence, step
+// counter and time are set first; files are written to the current directory.
+void ref_diagnostics(ref_sim *s, int nn, double time, double output_every) {
+  s->commondata.nn = nn;
+  s->commondata.time = time;
+  s->commondata.diagnostics_output_every = output_every;
+  diagnostics(&s->commondata, s->griddata);
+}
