@@ -11,6 +11,7 @@
 // H and M^2 at the nearest points; H^2, M^2^2 and |Lambda|^2 over "whole_domain" and
 // "sphere_R_gt_8" (points with r > 8).
 #include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -269,10 +270,22 @@ void write_header(FILE *f, const char *coord_names) {
   fprintf(f, "\n");
 }
 
+// One row "%.15e %.15e ...\n" appended to a buffer (std::to_chars gives the same digits as
+// printf's %.15e, correctly rounded, and runs several times faster).
+void append_row(std::string &buf, int ncols, const double *v) {
+  char tmp[40];
+  for (int k = 0; k < ncols; k++) {
+    if (k) buf.push_back(' ');
+    const auto r = std::to_chars(tmp, tmp + sizeof tmp, v[k], std::chars_format::scientific, 15);
+    buf.append(tmp, r.ptr);
+  }
+  buf.push_back('\n');
+}
+
 void write_row(FILE *f, int ncols, const double *v) {
-  fprintf(f, "%.15e", v[0]);
-  for (int k = 1; k < ncols; k++) fprintf(f, " %.15e", v[k]);
-  fprintf(f, "\n");
+  std::string b;
+  append_row(b, ncols, v);
+  fwrite(b.data(), 1, b.size(), f);
 }
 
 std::string rule_name(const Recipes &rc, int q, int u) {
@@ -445,10 +458,13 @@ int nearest(const commondata_struct *cd, const griddata_struct *gd, const REAL *
       if (!o) return BSSN_B200_EINVAL;
       fprintf(o, "# [time] = %.15e\n", cd->time);
       write_header(o, line == 0 ? "y" : "z");
+      std::string buf;
+      buf.reserve(v.size() * 72);
       for (size_t q = 0; q < v.size(); q++, at++) {
         const double row[3] = {v[q].c0, val(at, 0), val(at, 1)};
-        write_row(o, 1 + kNearestNum, row);
+        append_row(buf, 1 + kNearestNum, row);
       }
+      fwrite(buf.data(), 1, buf.size(), o);
       fclose(o);
     }
     for (int plane = 0; plane < 2; plane++) {
@@ -457,10 +473,13 @@ int nearest(const commondata_struct *cd, const griddata_struct *gd, const REAL *
       if (!o) return BSSN_B200_EINVAL;
       fprintf(o, "# [time] = %.15e\n", cd->time);
       write_header(o, plane == 0 ? "x y" : "y z");
+      std::string buf;
+      buf.reserve(v.size() * 96);
       for (size_t q = 0; q < v.size(); q++, at++) {
         const double row[4] = {v[q].c0, v[q].c1, val(at, 0), val(at, 1)};
-        write_row(o, 2 + kNearestNum, row);
+        append_row(buf, 2 + kNearestNum, row);
       }
+      fwrite(buf.data(), 1, buf.size(), o);
       fclose(o);
     }
   }
