@@ -447,6 +447,11 @@ def run_diagnostics(grid, args, reps: int = 3):
     n0 = grid.N[0] - 6
     samples = 1 + 4 * n0 + n0 * n2 + 2 * n0 * n1
     res["d2h_bytes_per_output"] = samples * 2 * 8 + 8 * 8
+    # initial data (Brill-Lindquist -> BSSN on the device, lambda^i, BCs)
+    t0 = time.perf_counter()
+    grid.lib.initial_data(C.byref(grid.cd), grid.gd)
+    torch.cuda.synchronize()
+    res["initial_data_ms"] = 1e3 * (time.perf_counter() - t0)
     res["reference_cuda_path_d2h_bytes_per_output"] = grid.y_n.numel() * 8
     if not args.no_cpu_baseline:
         try:
@@ -463,6 +468,9 @@ def run_diagnostics(grid, args, reps: int = 3):
                         t0 = time.perf_counter()
                         rg.diagnostics(1, 0.0, 1.0)
                         res["reference_ms_per_output"] = 1e3 * (time.perf_counter() - t0)
+                        t0 = time.perf_counter()
+                        rg.initial_data()
+                        res["reference_initial_data_ms"] = 1e3 * (time.perf_counter() - t0)
                     finally:
                         os.chdir(cwd)
                 rg.close()

@@ -66,17 +66,17 @@ void params_defaults(params_struct *p) {
 struct Coord {
   int sinh;
   double AMPL, SINHW;
-  double r(double xx0) const {
+  __host__ __device__ double r(double xx0) const {
     if (!sinh) return xx0;
     const double tmp0 = 1.0 / SINHW;
     return AMPL * (exp(tmp0 * xx0) - exp(-tmp0 * xx0)) / (exp(tmp0) - exp(-tmp0));
   }
-  double drdx0(double xx0) const {
+  __host__ __device__ double drdx0(double xx0) const {
     if (!sinh) return 1.0;
     const double tmp0 = 1.0 / SINHW;
     return AMPL * (exp(tmp0 * xx0) * tmp0 + exp(-tmp0 * xx0) * tmp0) / (exp(tmp0) - exp(-tmp0));
   }
-  void to_cart(double xx0, double xx1, double xx2, double out[3]) const {
+  __host__ __device__ void to_cart(double xx0, double xx1, double xx2, double out[3]) const {
     const double rr = r(xx0);
     const double tmp = rr * sin(xx1);
     out[0] = tmp * cos(xx2);
@@ -453,60 +453,78 @@ int cfl_dt(commondata_struct *cd, const params_struct *p, REAL *xx[3]) {
 // alpha = psi^-2), ADM -> BSSN in the Cartesian basis, then the basis change to the
 // reference-metric basis and rescaling (ADM_Initial_Data_Reader__BSSN_Converter.py:33-460),
 // lambda^i from centred FD of hDD on the interior, then extrapolation and inner BCs.
+struct BLData {
+  double m1, x1, y1, z1, m2, x2, y2, z2;
+};
+
+// Brill-Lindquist data at every point (InitialData_Cartesian.py:111-141) converted to the
+// rescaled BSSN variables (ADM_Initial_Data_Reader__BSSN_Converter.py:33-1181): ADM in
+// Cartesian gamma_ij = psi^4 delta_ij, K_ij = 0, alpha = psi^-2; gammabar_ij = (det
+// gamma)^(-1/3) gamma_ij transformed to the reference basis, h_ij = (gammabar_ij -
+// ghat_ij) / ReDD_ij, W = cf = (det gamma)^(-1/6). Every other gridfunction is zero
+// (lambda^i is set afterwards from finite differences of h_ij on the interior).
+__global__ void bl_initial_data_kernel(const GridDims g, const Coord c, const double *__restrict__ xx0,
+                                       const double *__restrict__ xx1, const double *__restrict__ xx2,
+                                       const BLData bl, double *__restrict__ y) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= g.ntot) return;
+  const int i2 = idx / g.s2;
+  const int rem = idx - i2 * g.s2;
+  const int i1 = rem / g.s1;
+  const int i0 = rem - i1 * g.s1;
+  const double a0 = xx0[i0], a1 = xx1[i1], a2 = xx2[i2];
+  double X[3];
+  c.to_cart(a0, a1, a2, X);
+  const double d1 = sqrt((X[0] - bl.x1) * (X[0] - bl.x1) + (X[1] - bl.y1) * (X[1] - bl.y1) +
+                         (X[2] - bl.z1) * (X[2] - bl.z1));
+  const double d2 = sqrt((X[0] - bl.x2) * (X[0] - bl.x2) + (X[1] - bl.y2) * (X[1] - bl.y2) +
+                         (X[2] - bl.z2) * (X[2] - bl.z2));
+  const double psi = (1.0 / 2.0) * bl.m1 / d1 + (1.0 / 2.0) * bl.m2 / d2 + 1;
+  const double psi4 = psi * psi * psi * psi;
+  const double detg = psi4 * psi4 * psi4;
+  const double alpha = 1.0 / sqrt(cbrt(detg));
+  const double gbar = psi4 * cbrt(1.0 / detg);  // diagonal of gammabar_ij (= 1 up to rounding)
+  const double cf = 1.0 / sqrt(cbrt(detg));
+  const double rr = c.r(a0), dr = c.drdx0(a0);
+  const double st = sin(a1), ct = cos(a1), sp_ = sin(a2), cp = cos(a2);
+  const double J[3][3] = {{dr * st * cp, rr * ct * cp, -rr * st * sp_},
+                          {dr * st * sp_, rr * ct * sp_, rr * st * cp},
+                          {dr * ct, -rr * st, 0.0}};
+  const double sf[3] = {dr, rr, rr * st};  // scale factors; ReDD_ij = sf_i sf_j
+  const double ghat[3] = {dr * dr, rr * rr, rr * rr * st * st};
+  const size_t n = (size_t)g.ntot;
+#pragma unroll
+  for (int gf = 0; gf < NUM_EVOL_GFS; gf++) y[gf * n + idx] = 0.0;
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = i; j < 3; j++, k++) {
+      double gg = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; a++) gg += J[a][i] * J[a][j] * gbar;
+      const double gh = (i == j) ? ghat[i] : 0.0;
+      y[(HDD00GF + k) * n + idx] = (gg - gh) / (sf[i] * sf[j]);
+    }
+  y[ALPHAGF * n + idx] = alpha;
+  y[CFGF * n + idx] = cf;
+}
+
 int bl_initial_data(const commondata_struct *cd, const params_struct *p, REAL *xx[3], const bc_struct *bc,
                     double *y_n, cudaStream_t s) {
+  (void)bc;
   Coord c;
   BSSN_TRY(coord_of(p, &c));
-  Variant v;
-  BSSN_TRY(variant_of(p, &v));
-  std::vector<double> hx[3];
-  BSSN_TRY(host_xx(p, xx, hx));
-  const int N0 = p->Nxx_plus_2NGHOSTS0, N1 = p->Nxx_plus_2NGHOSTS1, N2 = p->Nxx_plus_2NGHOSTS2;
-  const size_t ntot = (size_t)N0 * N1 * N2;
-  std::vector<double> h(ntot * NUM_EVOL_GFS, 0.0);
-  for (int i2 = 0; i2 < N2; i2++)
-    for (int i1 = 0; i1 < N1; i1++)
-      for (int i0 = 0; i0 < N0; i0++) {
-        const double xx0 = hx[0][i0], xx1 = hx[1][i1], xx2 = hx[2][i2];
-        double X[3];
-        c.to_cart(xx0, xx1, xx2, X);
-        const double d1 = sqrt((X[0] - cd->BH1_posn_x) * (X[0] - cd->BH1_posn_x) + (X[1] - cd->BH1_posn_y) * (X[1] - cd->BH1_posn_y) +
-                               (X[2] - cd->BH1_posn_z) * (X[2] - cd->BH1_posn_z));
-        const double d2 = sqrt((X[0] - cd->BH2_posn_x) * (X[0] - cd->BH2_posn_x) + (X[1] - cd->BH2_posn_y) * (X[1] - cd->BH2_posn_y) +
-                               (X[2] - cd->BH2_posn_z) * (X[2] - cd->BH2_posn_z));
-        const double psi = (1.0 / 2.0) * cd->BH1_mass / d1 + (1.0 / 2.0) * cd->BH2_mass / d2 + 1;
-        const double psi4 = psi * psi * psi * psi;
-        const double alpha = 1.0 / sqrt(cbrt(pow(psi, 12)));
-        // ADM (Cartesian): gamma_ij = psi^4 delta_ij, K_ij = 0 -> BSSN (Cartesian):
-        const double detg = psi4 * psi4 * psi4;
-        const double gbar_scale = cbrt(1.0 / detg);  // (det gamma)^(-1/3)
-        const double gbar = psi4 * gbar_scale;       // diagonal of gammabar_ij (= 1 up to rounding)
-        const double cf = 1.0 / sqrt(cbrt(detg));
-        // Basis change: gammabar^rfm_ij = J_ai J_bj gammabar^Cart_ab with J_ai = dx^a/dxx^i.
-        const double rr = c.r(xx0), dr = c.drdx0(xx0);
-        const double st = sin(xx1), ct = cos(xx1), sp_ = sin(xx2), cp = cos(xx2);
-        const double J[3][3] = {{dr * st * cp, rr * ct * cp, -rr * st * sp_},
-                                {dr * st * sp_, rr * ct * sp_, rr * st * cp},
-                                {dr * ct, -rr * st, 0.0}};
-        const double sf[3] = {dr, rr, rr * st};  // scale factors; ReDD_ij = sf_i sf_j
-        const double ghat[3] = {dr * dr, rr * rr, rr * rr * st * st};
-        const size_t idx = i0 + (size_t)N0 * (i1 + (size_t)N1 * i2);
-        int k = 0;
-        const int hslot[6] = {HDD00GF, HDD01GF, HDD02GF, HDD11GF, HDD12GF, HDD22GF};
-        for (int i = 0; i < 3; i++)
-          for (int j = i; j < 3; j++, k++) {
-            double g = 0.0;
-            for (int a = 0; a < 3; a++) g += J[a][i] * J[a][j] * gbar;
-            const double gh = (i == j) ? ghat[i] : 0.0;
-            h[idx + ntot * hslot[k]] = (g - gh) / (sf[i] * sf[j]);
-          }
-        h[idx + ntot * ALPHAGF] = alpha;
-        h[idx + ntot * CFGF] = cf;
-        // aDD, trK, vetU, betU, lambdaU (interior lambda set below) are zero for BL data.
-      }
-  BSSN_CUDA_TRY(cudaStreamSynchronize(s));
-  BSSN_CUDA_TRY(cudaMemcpy(y_n, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
-  (void)v;
+  for (int d = 0; d < 3; d++)
+    if (!xx[d]) {
+      set_error("initial data: xx[%d] is NULL", d);
+      return BSSN_B200_EINVAL;
+    }
+  const GridDims g = grid_dims(p);
+  const BLData bl{cd->BH1_mass, cd->BH1_posn_x, cd->BH1_posn_y, cd->BH1_posn_z,
+                  cd->BH2_mass, cd->BH2_posn_x, cd->BH2_posn_y, cd->BH2_posn_z};
+  bl_initial_data_kernel<<<(g.ntot + 127) / 128, 128, 0, s>>>(g, c, xx[0], xx[1], xx[2], bl, y_n);
+  BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
 

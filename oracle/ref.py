@@ -82,6 +82,7 @@ def _load(variant: str) -> C.CDLL:
     lib.ref_dV.restype = C.c_double
     lib.ref_dV.argtypes = [vp, ip, ip, ip]
     lib.ref_diagnostics.argtypes = [vp, ip, C.c_double, C.c_double]
+    lib.ref_initial_data.argtypes = [vp]
     lib.ref_destroy.argtypes = [vp]
     for f in ("ref_sizeof_commondata", "ref_sizeof_params", "ref_sizeof_bc_struct", "ref_sizeof_griddata",
               "ref_sizeof_innerpt", "ref_sizeof_outerpt", "ref_offsetof_params_Nxx0", "ref_offsetof_params_invdxx0",
@@ -184,6 +185,10 @@ class RefGrid:
         self.lib.ref_constraints(self.h, _dp(in_gfs), _dp(aux), _dp(diag))
         d = diag.reshape(ndiag, self.ntot)
         return np.stack([d[self.lib.ref_diag_index(k)] for k in range(3)])
+
+    def initial_data(self) -> None:
+        """Recompute the generated initial_data() into y_n."""
+        self.lib.ref_initial_data(self.h)
 
     def diagnostics(self, nn: int, time: float, output_every: float) -> None:
         """The generated diagnostics() driver at the present state (files in the current directory)."""

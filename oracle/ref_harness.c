@@ -195,3 +195,5 @@ void ref_diagnostics(ref_sim *s, int nn, double time, double output_every) {
   s->commondata.diagnostics_output_every = output_every;
   diagnostics(&s->commondata, s->griddata);
 }
+// The generated initial_data() (Brill-Lindquist -> BSSN, lambda^i, BCs) on this grid.
+void ref_initial_data(ref_sim *s) { initial_data(&s->commondata, s->griddata); }
