@@ -201,7 +201,9 @@ extern const REAL gridfunctions_f_infinity[NUM_EVOL_GFS];
 void commondata_struct_set_to_default(commondata_struct *commondata);
 void params_struct_set_to_default(commondata_struct *commondata, griddata_struct *griddata);
 
-/* numerical_grids_and_timestep.py:31-190 -- Nxx, dxx, invdxx, cell-centred xx[3] (allocated on device). */
+/* numerical_grids_and_timestep.py:31-190 -- Nxx, dxx, invdxx, cell-centred xx[3] (allocated on device).
+ * Nxx = Nx when all three entries are set (not -1), else the generated project's default
+ * (72, 12, 2) (two_blackholes_collide's Nxx_dict); then the convergence factor is applied. */
 void numerical_grid_params_Nxx_dxx_xx(const commondata_struct *commondata, params_struct *params, REAL *xx[3],
                                       const int Nx[3], const bool apply_convergence_factor_and_set_xxminmax_defaults);
 /* rfm_precompute.py:84-565 */

@@ -109,6 +109,11 @@ static int host_xx(const params_struct *p, REAL *const xx[3], std::vector<double
 int grid_params(const commondata_struct *cd, params_struct *p, REAL *xx[3], const int Nx[3], bool apply_defaults) {
   Coord c;
   BSSN_TRY(coord_of(p, &c));
+  // Default resolution of the generated project (two_blackholes_collide's Nxx_dict for
+  // Spherical and SinhSpherical), replaced by Nx when all three entries are set.
+  p->Nxx0 = 72;
+  p->Nxx1 = 12;
+  p->Nxx2 = 2;
   if (Nx != nullptr && Nx[0] != -1 && Nx[1] != -1 && Nx[2] != -1) {
     p->Nxx0 = Nx[0];
     p->Nxx1 = Nx[1];
