@@ -541,6 +541,7 @@ def emit_point_function(
     reg_capacity: int = 0,
     remat_first: bool = False,
     deriv_remat: bool = False,
+    order: str = "dfs",
 ) -> Tuple[str, Dict[str, int]]:
     """Emit `fname` and the constant `fname_SMEM_SLOTS`. With reg_capacity > 0 the values
     beyond that many live doubles go to shared-memory slots (SMEM(k), provided by the
@@ -548,8 +549,14 @@ def emit_point_function(
     the slot stride, i.e. the threads of a block)."""
     pk = PointKernel(symmetry_axes)
     pk.build(outputs, upwind_vec)
-    lines, nslots = (allocate_values(dfs_order(pk.lines), reg_capacity, remat_first, deriv_remat)
-                     if reg_capacity > 0 else (pk.lines, 0))
+    if reg_capacity > 0:
+        # Statement order: "dfs" completes one output at a time (dfs_order); "sched" keeps the
+        # greedy live-range schedule; "sched_dfs" reschedules the dfs order greedily.
+        ordered = {"dfs": lambda: dfs_order(pk.lines), "sched": lambda: pk.lines,
+                   "sched_dfs": lambda: schedule_lines(dfs_order(pk.lines))}[order]()
+        lines, nslots = allocate_values(ordered, reg_capacity, remat_first, deriv_remat)
+    else:
+        lines, nslots = pk.lines, 0
     body = "\n".join("  " + ln for ln in lines)
     head = f"// {comment}\n" if comment else ""
     code = (

@@ -45,14 +45,16 @@ ADJ_RHS_GROUPS = [
     ["betU0", "betU1", "betU2", "lambdaU0", "lambdaU1", "lambdaU2"],
 ]
 REG_CAPACITY = 90
-# Per group: (remat_first, deriv_remat) of the value allocator -- whether register eviction
-# prefers recomputable values (stencil loads, rfm, parameters) and whether finite
-# differences are recomputed from their stencils instead of kept in a slot. Chosen by
-# timing every group kernel of SinhSpherical 256x64x32 on a B200 under each allocation
-# (and 64/128 threads per block); lower register budgets with forced occupancy were
+# Per group: (remat_first, deriv_remat, statement order) of the value allocator --
+# whether register eviction prefers recomputable values (stencil loads, rfm, parameters),
+# whether finite differences are recomputed from their stencils instead of kept in a slot,
+# and the statement order ("dfs": one output at a time; "sched": greedy live-range
+# schedule; "sched_dfs": the dfs order rescheduled greedily). Chosen by timing every group
+# kernel of SinhSpherical 256x64x32 on a B200 under each allocation, order and block size
+# (nrpy_b200/codegen/tune_groups.py); lower register budgets with forced occupancy were
 # slower in every group (local-memory spills).
-RICCI_ALLOC = [(True, True), (True, True)]
-RHS_ALLOC = [(True, False), (True, False)]
+RICCI_ALLOC = [(True, True, "sched_dfs"), (True, False, "sched_dfs")]
+RHS_ALLOC = [(True, False, "dfs"), (True, False, "sched")]
 # Threads per block of a group kernel: 128, or 64 when two 128-thread blocks of its
 # shared-memory slots would not fit in the 227 KB of one SM.
 SMEM_PER_SM = 227 * 1024
@@ -102,11 +104,11 @@ def generate_variant(tag: str) -> None:
     structs = [f"template <int G> struct RicciGroup_{tag};\n", f"template <int G> struct RhsGroup_{tag};\n"]
     for g, names in enumerate(RICCI_GROUPS):
         fname = f"ricci_point_{tag}_g{g}"
-        remat_first, deriv_remat = RICCI_ALLOC[g]
+        remat_first, deriv_remat, order = RICCI_ALLOC[g]
         code, st = emit_point_function(
             fname, [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
             comment=f"Rbar_ij {names}, {coord} (symmetry_axes='{sym}'): Ricci_eval.py:27-167",
-            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat,
+            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
         )
         parts.append(code)
         stats[f"ricci_g{g}"] = st
@@ -114,11 +116,11 @@ def generate_variant(tag: str) -> None:
                                      st["smem_slots"]))
     for g, names in enumerate(RHS_GROUPS):
         fname = f"rhs_point_{tag}_g{g}"
-        remat_first, deriv_remat = RHS_ALLOC[g]
+        remat_first, deriv_remat, order = RHS_ALLOC[g]
         code, st = emit_point_function(
             fname, [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU, symmetry_axes=sym,
             comment=f"BSSN RHS + KO (CAKO) of {names}, {coord} (symmetry_axes='{sym}'): rhs_eval.py:122-220",
-            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat,
+            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
         )
         parts.append(code)
         stats[f"rhs_g{g}"] = st
@@ -156,8 +158,8 @@ def generate_variant(tag: str) -> None:
     hdr = (
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', 4th-order FD, KO (CAKO).\n"
-        f"// Register budget {REG_CAPACITY} values; allocation (remat_first, deriv_remat): Ricci {RICCI_ALLOC}, "
-        f"RHS {RHS_ALLOC}.\n"
+        f"// Register budget {REG_CAPACITY} values; allocation (remat_first, deriv_remat, order): Ricci "
+        f"{RICCI_ALLOC}, RHS {RHS_ALLOC}.\n"
         f"// Per point: {stats}\n"
         "#pragma once\n\n"
     )

@@ -4,6 +4,7 @@ Code-generation-time tuning tool (the output-group split and the per-group alloc
 flags in generate.py come from its measurements). Three steps:
 
   python -m nrpy_b200.codegen.tune_groups generate   # needs nrpy (equation modules)
+  python -m nrpy_b200.codegen.tune_groups generate-orders  # present groups x statement orders
   python -m nrpy_b200.codegen.tune_groups compile    # nvcc, sm_100a, no GPU needed
   python -m nrpy_b200.codegen.tune_groups run        # on a B200; prints one line per kernel
 
@@ -182,6 +183,43 @@ def generate() -> None:
         print(gname, flush=True)
 
 
+ORDER_GROUPS = ["ricci_012", "ricci_345", "rhs_a_g1", "rhs_g2"]
+ORDERS = ["dfs", "sched", "sched_dfs"]
+
+
+def generate_orders() -> None:
+    """The present groups under each statement order and the two recompute-first allocations."""
+    from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen.emit_cuda import emit_point_function
+
+    be.setup_nrpy("")
+    rhs, betaU = be.rhs_exprs("SinhSpherical")
+    ricci = be.ricci_exprs("SinhSpherical")
+    OUT.mkdir(parents=True, exist_ok=True)
+    for gname in ORDER_GROUPS:
+        kind, names = CANDIDATES[gname]
+        src, uv = (ricci, None) if kind == "ricci" else (rhs, betaU)
+        parts, wrappers, calls = ["#pragma once\n"], [], []
+        for order in ORDERS:
+            for rf, dr in ((True, True), (True, False)):
+                fname = f"{gname}_{order}_r{int(rf)}_d{int(dr)}"
+                code, st = emit_point_function(fname, [(f"out[{i}]", src[n]) for i, n in enumerate(names)],
+                                               upwind_vec=uv, reg_capacity=90, remat_first=rf, deriv_remat=dr,
+                                               order=order)
+                parts.append(code)
+                slots = max(st["smem_slots"], 1)
+                wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
+                                f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
+                nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
+                calls.append(f'  run<{nt}, 1, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+        tag = f"order_{gname}"
+        (OUT / f"{tag}.cuh").write_text("\n".join(parts))
+        head, main = HARNESS_HEAD.replace("GROUP", tag).split("int main() {")
+        (OUT / f"{tag}.cu").write_text(head + "\n".join(wrappers) + "\nint main() {" + main + "\n".join(calls)
+                                        + "\n  return 0;\n}\n")
+        print(tag, flush=True)
+
+
 def compile_all(jobs: int) -> None:
     from nrpy_b200.build import nvcc
 
@@ -220,12 +258,14 @@ def summarize(path: str) -> None:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["generate", "compile", "run", "summarize"])
+    ap.add_argument("step", choices=["generate", "generate-orders", "compile", "run", "summarize"])
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--log", default=None)
     a = ap.parse_args()
     if a.step == "generate":
         generate()
+    elif a.step == "generate-orders":
+        generate_orders()
     elif a.step == "compile":
         compile_all(a.jobs)
     elif a.step == "run":
