@@ -31,7 +31,7 @@ from typing import Callable, Dict, List, Sequence, Tuple
 import sympy as sp
 
 from .bssn_exprs import GF_ORDER, RBAR_ORDER
-from .emit_cuda import GF_INDEX, RBAR_INDEX, PointKernel, allocate_values, dfs_order, parse_deriv
+from .emit_cuda import GF_INDEX, RBAR_INDEX, PointKernel, allocate_values, dfs_order, parse_deriv, schedule_lines
 
 KIND_CODE = {"C": 0, "D": 1, "DD": 2, "upD": 3, "KOD": 4}
 
@@ -112,7 +112,7 @@ def leaf_table(names: Sequence[str]) -> List[Tuple[str, int, int, int, int]]:
 
 def emit_vjp_function(fname: str, outputs: Sequence[sp.Expr], row_of: Dict[str, int], upwind_vec=None,
                       symmetry_axes: str = "", comment: str = "", reg_capacity: int = 64, remat_first: bool = False,
-                      deriv_remat: bool = False):
+                      deriv_remat: bool = False, order: str = "dfs"):
     """Emit the VJP of `outputs` as `fname(ctx, sm)` plus `fname_SMEM_SLOTS`.
 
     Gridfunction and derivative leaf adjoints go to OUT(row_of[name]); Rbar_ij adjoints
@@ -124,7 +124,9 @@ def emit_vjp_function(fname: str, outputs: Sequence[sp.Expr], row_of: Dict[str, 
         lhs = f"OUTR({RBAR_INDEX[name]})" if name in RBAR_INDEX else f"OUT({row_of[name]})"
         outs.append((lhs, leaf_adj[name]))
     pk.build_program(stmts, outs, upwind_vec)
-    lines, nslots = allocate_values(dfs_order(pk.lines), reg_capacity, remat_first, deriv_remat)
+    ordered = {"dfs": lambda: dfs_order(pk.lines), "sched": lambda: pk.lines,
+               "sched_dfs": lambda: schedule_lines(dfs_order(pk.lines))}[order]()
+    lines, nslots = allocate_values(ordered, reg_capacity, remat_first, deriv_remat)
     body = "\n".join("  " + ln for ln in lines)
     head = f"// {comment}\n" if comment else ""
     code = (
