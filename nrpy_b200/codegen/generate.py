@@ -27,7 +27,7 @@ VARIANTS = {
 
 
 # Output groups: each group is one kernel (its own CSE); groups trade recomputed shared
-# subexpressions for fewer live values per thread. Values beyond REG_CAPACITY live doubles
+# subexpressions for fewer live values per thread. Values beyond each group's register budget
 # go to per-thread shared-memory slots. The split was chosen by timing every candidate
 # group kernel of SinhSpherical 256x64x32 on a B200 (Ricci: 1x6, 2x3, 3x2 and 6x1 outputs;
 # RHS: the gauge/metric/extrinsic-curvature outputs together or in two or three parts).
@@ -44,7 +44,6 @@ ADJ_RHS_GROUPS = [
     ["alpha", "cf", "hDD00", "hDD01", "hDD02", "hDD11", "hDD12", "hDD22", "trK", "vetU0", "vetU1", "vetU2"],
     ["betU0", "betU1", "betU2", "lambdaU0", "lambdaU1", "lambdaU2"],
 ]
-REG_CAPACITY = 90
 # Per group: (remat_first, deriv_remat, statement order) of the value allocator --
 # whether register eviction prefers recomputable values (stencil loads, rfm, parameters),
 # whether finite differences are recomputed from their stencils instead of kept in a slot,
@@ -55,6 +54,11 @@ REG_CAPACITY = 90
 # slower in every group (local-memory spills).
 RICCI_ALLOC = [(True, True, "sched_dfs"), (True, False, "sched_dfs")]
 RHS_ALLOC = [(True, False, "dfs"), (True, False, "sched")]
+# Per group register budget (values kept in registers), from the same timing sweep: the
+# Ricci groups gain from keeping more values in registers (fewer slots leave more L1 for
+# stencil loads) even with a few local-memory spills.
+RICCI_CAPS = [120, 140]
+RHS_CAPS = [72, 80]
 # Threads per block of a group kernel: 128, or 64 when two 128-thread blocks of its
 # shared-memory slots would not fit in the 227 KB of one SM.
 SMEM_PER_SM = 227 * 1024
@@ -107,10 +111,11 @@ def generate_variant(tag: str) -> None:
     for g, names in enumerate(RICCI_GROUPS):
         fname = f"ricci_point_{tag}_g{g}"
         remat_first, deriv_remat, order = RICCI_ALLOC[g]
+        cap = RICCI_CAPS[g]
         code, st = emit_point_function(
             fname, [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
             comment=f"Rbar_ij {names}, {coord} (symmetry_axes='{sym}'): Ricci_eval.py:27-167",
-            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+            reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
         )
         parts.append(code)
         stats[f"ricci_g{g}"] = st
@@ -119,10 +124,11 @@ def generate_variant(tag: str) -> None:
     for g, names in enumerate(RHS_GROUPS):
         fname = f"rhs_point_{tag}_g{g}"
         remat_first, deriv_remat, order = RHS_ALLOC[g]
+        cap = RHS_CAPS[g]
         code, st = emit_point_function(
             fname, [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU, symmetry_axes=sym,
             comment=f"BSSN RHS + KO (CAKO) of {names}, {coord} (symmetry_axes='{sym}'): rhs_eval.py:122-220",
-            reg_capacity=REG_CAPACITY, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+            reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
         )
         parts.append(code)
         stats[f"rhs_g{g}"] = st
@@ -160,8 +166,8 @@ def generate_variant(tag: str) -> None:
     hdr = (
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', 4th-order FD, KO (CAKO).\n"
-        f"// Register budget {REG_CAPACITY} values; allocation (remat_first, deriv_remat, order): Ricci "
-        f"{RICCI_ALLOC}, RHS {RHS_ALLOC}.\n"
+        f"// Register budgets Ricci {RICCI_CAPS}, RHS {RHS_CAPS} values; allocation (remat_first, deriv_remat, "
+        f"order): Ricci {RICCI_ALLOC}, RHS {RHS_ALLOC}.\n"
         f"// Per point: {stats}\n"
         "#pragma once\n\n"
     )

@@ -5,6 +5,7 @@ flags in generate.py come from its measurements). Three steps:
 
   python -m nrpy_b200.codegen.tune_groups generate   # needs nrpy (equation modules)
   python -m nrpy_b200.codegen.tune_groups generate-orders  # present groups x statement orders
+  python -m nrpy_b200.codegen.tune_groups generate-caps    # present groups x register budgets
   python -m nrpy_b200.codegen.tune_groups compile    # nvcc, sm_100a, no GPU needed
   python -m nrpy_b200.codegen.tune_groups run        # on a B200; prints one line per kernel
 
@@ -220,6 +221,41 @@ def generate_orders() -> None:
         print(tag, flush=True)
 
 
+def generate_caps(caps) -> None:
+    """The present groups with their chosen allocation and order (generate.py) at several
+    register budgets."""
+    from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen.emit_cuda import emit_point_function
+    from nrpy_b200.codegen.generate import RHS_ALLOC, RICCI_ALLOC
+
+    be.setup_nrpy("")
+    rhs, betaU = be.rhs_exprs("SinhSpherical")
+    ricci = be.ricci_exprs("SinhSpherical")
+    OUT.mkdir(parents=True, exist_ok=True)
+    chosen = dict(zip(ORDER_GROUPS, list(RICCI_ALLOC) + list(RHS_ALLOC)))
+    for gname in ORDER_GROUPS:
+        kind, names = CANDIDATES[gname]
+        src, uv = (ricci, None) if kind == "ricci" else (rhs, betaU)
+        rf, dr, order = chosen[gname]
+        parts, wrappers, calls = ["#pragma once\n"], [], []
+        for cap in caps:
+            fname = f"{gname}_c{cap}"
+            code, st = emit_point_function(fname, [(f"out[{i}]", src[n]) for i, n in enumerate(names)],
+                                           upwind_vec=uv, reg_capacity=cap, remat_first=rf, deriv_remat=dr, order=order)
+            parts.append(code)
+            slots = max(st["smem_slots"], 1)
+            wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
+                            f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
+            nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
+            calls.append(f'  run<{nt}, 1, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+        tag = f"caps_{gname}"
+        (OUT / f"{tag}.cuh").write_text("\n".join(parts))
+        head, main = HARNESS_HEAD.replace("GROUP", tag).split("int main() {")
+        (OUT / f"{tag}.cu").write_text(head + "\n".join(wrappers) + "\nint main() {" + main + "\n".join(calls)
+                                        + "\n  return 0;\n}\n")
+        print(tag, flush=True)
+
+
 def compile_all(jobs: int) -> None:
     from nrpy_b200.build import nvcc
 
@@ -258,7 +294,8 @@ def summarize(path: str) -> None:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["generate", "generate-orders", "compile", "run", "summarize"])
+    ap.add_argument("step", choices=["generate", "generate-orders", "generate-caps", "compile", "run", "summarize"])
+    ap.add_argument("--caps", default="72,80,90,100")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--log", default=None)
     a = ap.parse_args()
@@ -266,6 +303,8 @@ if __name__ == "__main__":
         generate()
     elif a.step == "generate-orders":
         generate_orders()
+    elif a.step == "generate-caps":
+        generate_caps([int(c) for c in a.caps.split(",")])
     elif a.step == "compile":
         compile_all(a.jobs)
     elif a.step == "run":
