@@ -57,7 +57,7 @@ RHS_ALLOC = [(True, False, "dfs"), (True, False, "sched")]
 # Per group register budget (values kept in registers), from the same timing sweep: the
 # Ricci groups gain from keeping more values in registers (fewer slots leave more L1 for
 # stencil loads) even with a few local-memory spills.
-RICCI_CAPS = [120, 140]
+RICCI_CAPS = [160, 150]
 RHS_CAPS = [72, 80]
 # Threads per block of a group kernel: 128, or 64 when two 128-thread blocks of its
 # shared-memory slots would not fit in the 227 KB of one SM.
