@@ -72,8 +72,10 @@ ADJOINT_VARIANTS = ["sph_3d"]
 # VJP kernels run 64 threads per block; recompute-first eviction and rematerialized finite
 # differences shrink the slot arrays of the largest group from 250 to 199 values (2 blocks
 # per SM instead of 1): the 200-step backward of the 128x32x32 workload went from 3.42 s to
-# 2.84 s on a B200 (a 90-value budget gave 2.84 s with more spills).
-ADJ_REG_CAPACITY = 64
+# 2.84 s on a B200 (a 90-value budget gave 2.84 s with more spills). Under the "sched_dfs"
+# order, budgets of 64/90/120/150/180/210/240 values ran the backward in 2.65/2.61/2.56/
+# 2.51/2.55/2.54/2.83 s; at 150 the largest group (rhs_g2) keeps 99 slots instead of 193.
+ADJ_REG_CAPACITY = 150
 # The greedy reschedule of the dfs order ("sched_dfs") ran the backward in 2.64 s ("dfs": 2.75 s,
 # "sched": 3.33 s).
 ADJ_REMAT = dict(remat_first=True, deriv_remat=True, order="sched_dfs")
