@@ -140,10 +140,33 @@ static dim3 interior_grid(const GridDims &g, int by = BY) {
   const int i2 = NGHOSTS + blockIdx.z;                    \
   if (i0 >= g.N0 - NGHOSTS || i1 >= g.N1 - NGHOSTS) return;
 
+// Group-kernel block geometry: TX points along i0, NT / (TX * TZ) along i1 and TZ along i2.
+#ifndef BSSN_TILE_X
+#define BSSN_TILE_X 32
+#endif
+#ifndef BSSN_TILE_Z
+#define BSSN_TILE_Z 1
+#endif
+constexpr int TX = BSSN_TILE_X, TZ = BSSN_TILE_Z;
+
+static dim3 group_block(int nt) { return dim3(TX, nt / (TX * TZ), TZ); }
+
+static dim3 group_grid(const GridDims &g, int nt) {
+  const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
+  const int ty = nt / (TX * TZ);
+  return dim3((n0 + TX - 1) / TX, (n1 + ty - 1) / ty, (n2 + TZ - 1) / TZ);
+}
+
+#define GROUP_INDEX_OR_RETURN(g)                                        \
+  const int i0 = NGHOSTS + blockIdx.x * blockDim.x + threadIdx.x;       \
+  const int i1 = NGHOSTS + blockIdx.y * blockDim.y + threadIdx.y;       \
+  const int i2 = NGHOSTS + blockIdx.z * blockDim.z + threadIdx.z;       \
+  if (i0 >= g.N0 - NGHOSTS || i1 >= g.N1 - NGHOSTS || i2 >= g.N2 - NGHOSTS) return;
+
 template <typename T>
 __device__ __forceinline__ volatile T *thread_slots() {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + blockDim.x * threadIdx.y);
+  return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z));
 }
 
 template <Variant V, int G, typename T, int NTB>
@@ -162,7 +185,7 @@ template <Variant V, int G, typename T>
 __global__ void __launch_bounds__(RicciG<V, G>::NT, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
                                                           const double *__restrict__ in, double *__restrict__ aux) {
   volatile T *sm = thread_slots<T>();
-  INTERIOR_INDEX_OR_RETURN(g);
+  GROUP_INDEX_OR_RETURN(g);
   ricci_body<V, G, T, RicciG<V, G>::NT>(g, rfm, in, aux, i0, i1, i2, sm);
 }
 
@@ -172,7 +195,7 @@ __global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_kernel(const GridDims g
                                                         double *__restrict__ rhs) {
   using Grp = RhsG<V, G>;
   volatile T *sm = thread_slots<T>();
-  INTERIOR_INDEX_OR_RETURN(g);
+  GROUP_INDEX_OR_RETURN(g);
   PointCtx ctx = make_ctx(g, rfm, in, aux, i0, i1, i2);
   ctx.eta = pp.eta;
   ctx.KreissOliger_strength_gauge = pp.ko_gauge;
@@ -321,7 +344,7 @@ __global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_fused_kernel(const Grid
                                                               const double *__restrict__ aux, const StageBuffers b,
                                                               double *__restrict__ krhs, const double dt) {
   volatile T *sm = thread_slots<T>();
-  INTERIOR_INDEX_OR_RETURN(g);
+  GROUP_INDEX_OR_RETURN(g);
   fused_body<V, T, STAGE, G, RhsG<V, G>::NT>(g, rfm, pp, aux, b, krhs, dt, i0, i1, i2, sm);
 }
 
@@ -371,7 +394,7 @@ static int launch_ricci_group(const GridDims &g, const RfmArrays &rfm, const dou
   using Grp = RicciG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(ricci_kernel<V, G, T>, sb));
-  ricci_kernel<V, G, T><<<interior_grid(g, Grp::NT / BX), dim3(BX, Grp::NT / BX), sb, s>>>(g, rfm, in, aux);
+  ricci_kernel<V, G, T><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, in, aux);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -399,7 +422,7 @@ static int launch_rhs_group(const GridDims &g, const RfmArrays &rfm, const PhysP
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(rhs_kernel<V, T, G>, sb));
-  rhs_kernel<V, T, G><<<interior_grid(g, Grp::NT / BX), dim3(BX, Grp::NT / BX), sb, s>>>(g, rfm, pp, aux, in, rhs);
+  rhs_kernel<V, T, G><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, pp, aux, in, rhs);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -452,7 +475,7 @@ static int launch_fused_group(const GridDims &g, const RfmArrays &rfm, const Phy
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(rhs_fused_kernel<V, T, STAGE, G>, sb));
-  rhs_fused_kernel<V, T, STAGE, G><<<interior_grid(g, Grp::NT / BX), dim3(BX, Grp::NT / BX), sb, s>>>(g, rfm, pp, aux, b,
+  rhs_fused_kernel<V, T, STAGE, G><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, pp, aux, b,
                                                                                               krhs, dt);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
