@@ -277,6 +277,7 @@ def main():
     # ---------------- end-to-end through the public API with host buffers
     e2e = None if args.no_e2e else run_e2e(grid, args, y0)
     diag = None if (args.no_diag or rank != 0) else run_diagnostics(grid, args)
+    ckpt = None if (args.no_diag or rank != 0) else run_checkpoint(grid, args)
     grid_dt = grid.dt
     grid.free_stepper()
     grid.close()
@@ -319,6 +320,7 @@ def main():
             "batched": batched,
             "differentiation": differentiation,
             "diagnostics": diag,
+            "checkpoint": ckpt,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -471,6 +473,71 @@ def run_diagnostics(grid, args, reps: int = 3):
                         t0 = time.perf_counter()
                         rg.initial_data()
                         res["reference_initial_data_ms"] = 1e3 * (time.perf_counter() - t0)
+                    finally:
+                        os.chdir(cwd)
+                rg.close()
+                res["reference_cores"] = os.cpu_count()
+        except Exception as e:  # noqa: BLE001
+            res["reference_unavailable"] = str(e)
+    return res
+
+
+def run_checkpoint(grid, args, reps: int = 3):
+    """write_checkpoint / read_checkpoint of the bench grid's state (the reference's file format,
+    246 MB at 256x64x64): wall time per call, the restored state checked bit-for-bit; beside it
+    the reference's own write_checkpoint / read_checkpoint (checkpoint-enabled project, same
+    grid size) on the host cores."""
+    import torch
+
+    cwd = os.getcwd()
+    res = {}
+    y_saved = grid.y_n.clone()
+    clock = (grid.cd.nn, grid.cd.time, grid.cd.t_0, grid.cd.nn_0)
+    every = grid.cd.time if grid.cd.time > 0 else 1.0
+    with tempfile.TemporaryDirectory() as d:
+        os.chdir(d)
+        try:
+            wt = []
+            for _ in range(reps):  # each write goes to a new file, as the reference's below
+                for f in os.listdir(d):
+                    os.remove(os.path.join(d, f))
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                grid.write_checkpoint(every)
+                wt.append(1e3 * (time.perf_counter() - t0))
+            res["write_ms"] = float(np.median(wt))
+            files = os.listdir(d)
+            res["file_bytes"] = os.path.getsize(os.path.join(d, files[0])) if files else 0
+            grid.y_n.zero_()
+            rt = []
+            for _ in range(reps):
+                t0 = time.perf_counter()
+                grid.read_checkpoint()
+                torch.cuda.synchronize()
+                rt.append(1e3 * (time.perf_counter() - t0))
+            res["read_ms"] = float(np.median(rt))
+            res["restored_bitwise"] = bool(torch.equal(grid.y_n, y_saved))
+        finally:
+            os.chdir(cwd)
+    grid.cd.nn, grid.cd.time, grid.cd.t_0, grid.cd.nn_0 = clock
+    grid.y_n.copy_(y_saved)
+    del y_saved
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+
+            if ref.available("sph3dck"):
+                rg = ref.RefGrid("sph3dck", NXX, 7.5)
+                with tempfile.TemporaryDirectory() as d:
+                    os.chdir(d)
+                    try:
+                        rg.set_clock(1, rg.dt)
+                        t0 = time.perf_counter()
+                        rg.write_checkpoint(rg.dt)
+                        res["reference_write_ms"] = 1e3 * (time.perf_counter() - t0)
+                        t0 = time.perf_counter()
+                        rg.read_checkpoint()
+                        res["reference_read_ms"] = 1e3 * (time.perf_counter() - t0)
                     finally:
                         os.chdir(cwd)
                 rg.close()

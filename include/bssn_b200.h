@@ -398,6 +398,63 @@ int bssn_b200_adjoint_destroy(bssn_b200_adjoint *adj);
  * kept by the library per grid and reused). */
 int bssn_b200_diagnostics(commondata_struct *commondata, griddata_struct *griddata, void *stream);
 
+/* ---- checkpoint / restart (checkpointing.py:15-470) ----
+ * The file is checkpoint-conv_factor%.2f.dat (convergence_factor) in the current directory, byte for
+ * byte in the format of the generated write_checkpoint/read_checkpoint of a project that registers
+ * checkpointing, so either side can resume the other's file:
+ *   bssn_b200_checkpoint_commondata (that project's commondata_struct), then per grid:
+ *   params_struct, int count, int indices[count], REAL data[count][NUM_EVOL_GFS] (point-major;
+ *   every point of the grid, indices 0..ntot-1, as the single-patch writer selects them).
+ * Registering checkpointing adds the REAL CodeParameter checkpoint_every to commondata_struct
+ * (checkpointing.py:253-255); the generated struct lists REAL fields by name, which puts it after
+ * KreissOliger_strength_nongauge. This library's commondata_struct is the layout of a project
+ * without it, so the cadence is an argument here and no drop-in named write_checkpoint or
+ * read_checkpoint is exported (its commondata argument would have the other layout). */
+typedef struct {
+  REAL BH1_mass;
+  REAL BH1_posn_x;
+  REAL BH1_posn_y;
+  REAL BH1_posn_z;
+  REAL BH2_mass;
+  REAL BH2_posn_x;
+  REAL BH2_posn_y;
+  REAL BH2_posn_z;
+  REAL CFL_FACTOR;
+  REAL KreissOliger_strength_gauge;
+  REAL KreissOliger_strength_nongauge;
+  REAL checkpoint_every;
+  REAL convergence_factor;
+  REAL diagnostics_output_every;
+  REAL dt;
+  REAL eta;
+  REAL t_0;
+  REAL t_final;
+  REAL time;
+  struct timespec start_wallclock_time;
+  char outer_bc_type[50];
+  int NUMGRIDS;
+  int nn;
+  int nn_0;
+  int output_progress_every;
+} bssn_b200_checkpoint_commondata;
+
+/* write_checkpoint (checkpointing.py:246-470). Writes only on checkpoint steps, as the reference:
+ * checkpoint_every > 0 and |round(time/checkpoint_every)*checkpoint_every - time| < dt/2. Returns 1
+ * when the file was written, 0 when this is not a checkpoint step, a negative code on failure (the
+ * reference exits instead). The state is read from each grid's device y_n_gfs; the packing into
+ * point-major order runs on the GPU, in chunks, overlapped with the file writes. */
+int bssn_b200_write_checkpoint(const commondata_struct *commondata, REAL checkpoint_every,
+                               const griddata_struct *griddata, void *stream);
+/* read_checkpoint (checkpointing.py:15-243). Returns 0 when the file does not exist, 1 when it was
+ * read, a negative code on failure (the reference exits instead). commondata is overwritten with the
+ * file's values, then t_0 = time and nn_0 = nn; checkpoint_every (may be NULL) receives the file's
+ * cadence. griddata == NULL reads only commondata (to rebuild the grids first). Otherwise each grid's
+ * saved params must match its Nxx_plus_2NGHOSTS* and CoordSystem_hash, count must lie in [0, ntot] and
+ * every index in [0, ntot); y_n_gfs (device, already allocated) is zeroed and the saved points are
+ * scattered into it on the GPU. */
+int bssn_b200_read_checkpoint(commondata_struct *commondata, REAL *checkpoint_every, griddata_struct *griddata,
+                              void *stream);
+
 /* Instrumentation: kernels launched by this library since it was loaded (each graph replay
  * counts its kernel nodes), and a launch of only the interior RHS + RK-update + projection
  * kernel of RK4 stage `stage` (1..4) of grid 0, used to time the dominant kernel alone.

@@ -20,7 +20,7 @@ BUILD = PKG / "_build"
 LIB = PKG / "libbssn_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["abi.cu", "setup.cu", "pointwise.cu", "boundary.cu", "mol.cu", "reductions.cu", "batch.cu",
-           "adjoint.cu", "diagnostics.cu"]
+           "adjoint.cu", "diagnostics.cu", "checkpoint.cu"]
 
 
 def nvcc() -> str:

@@ -232,6 +232,28 @@ class BSSNGrid:
         cd.diagnostics_output_every = float(output_every)
         L.check(self.lib.bssn_b200_diagnostics(C.byref(cd), self.gd, self.stream))
 
+    # ------------------------------------------------------------------ checkpoint / restart
+    def write_checkpoint(self, checkpoint_every: float) -> bool:
+        """write_checkpoint of a project that registers checkpointing: on checkpoint steps (time
+        within dt/2 of a multiple of checkpoint_every > 0) checkpoint-conv_factor%.2f.dat is written
+        to the current directory in the reference's format. Returns whether it was written."""
+        rc = self.lib.bssn_b200_write_checkpoint(C.byref(self.cd), float(checkpoint_every), self.gd, self.stream)
+        if rc < 0:
+            L.check(rc)
+        return rc == 1
+
+    def read_checkpoint(self) -> Optional[float]:
+        """read_checkpoint: restore commondata (time, nn, dt, ...; then t_0 = time, nn_0 = nn) and
+        y_n from checkpoint-conv_factor%.2f.dat in the current directory. The grid must have the
+        saved size and coordinate system. Returns the file's checkpoint_every, or None when there
+        is no checkpoint file."""
+        every = L.REAL()
+        rc = self.lib.bssn_b200_read_checkpoint(C.byref(self.cd), C.byref(every), self.gd, self.stream)
+        if rc < 0:
+            L.check(rc)
+        self.free_stepper()  # a captured graph bakes in dt
+        return every.value if rc == 1 else None
+
     # ------------------------------------------------------------------ time stepping
     def MoL_step_forward_in_time(self, mode: int = 1, mixed: bool = False, nsteps: int = 1) -> None:
         for _ in range(nsteps):

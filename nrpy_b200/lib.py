@@ -50,6 +50,20 @@ class CommondataStruct(C.Structure):
     ]
 
 
+class CheckpointCommondata(C.Structure):
+    """commondata_struct of a project that registers checkpointing (checkpoint files begin with it)."""
+    _fields_ = [
+        ("BH1_mass", REAL), ("BH1_posn_x", REAL), ("BH1_posn_y", REAL), ("BH1_posn_z", REAL),
+        ("BH2_mass", REAL), ("BH2_posn_x", REAL), ("BH2_posn_y", REAL), ("BH2_posn_z", REAL),
+        ("CFL_FACTOR", REAL), ("KreissOliger_strength_gauge", REAL),
+        ("KreissOliger_strength_nongauge", REAL), ("checkpoint_every", REAL), ("convergence_factor", REAL),
+        ("diagnostics_output_every", REAL), ("dt", REAL), ("eta", REAL), ("t_0", REAL),
+        ("t_final", REAL), ("time", REAL), ("start_wallclock_time", Timespec),
+        ("outer_bc_type", C.c_char * 50), ("NUMGRIDS", C.c_int), ("nn", C.c_int), ("nn_0", C.c_int),
+        ("output_progress_every", C.c_int),
+    ]
+
+
 class ParamsStruct(C.Structure):
     _fields_ = [
         ("AMPL", REAL), ("Cart_originx", REAL), ("Cart_originy", REAL), ("Cart_originz", REAL),
@@ -195,6 +209,8 @@ SIGNATURES = [
     ("bssn_b200_adjoint_step_vjp", C.c_int, [V, PR, PR]),
     ("bssn_b200_adjoint_id_vjp", C.c_int, [V, PR, C.POINTER(C.c_double)]),
     ("bssn_b200_adjoint_destroy", C.c_int, [V]),
+    ("bssn_b200_write_checkpoint", C.c_int, [PCD, REAL, PGD, V]),
+    ("bssn_b200_read_checkpoint", C.c_int, [PCD, PR, PGD, V]),
     ("bssn_b200_memcpy", C.c_int, [V, V, C.c_size_t, C.c_int]),
     ("bssn_b200_device_synchronize", C.c_int, []),
 ]

@@ -20,6 +20,7 @@ Variants
   sphaxi : Spherical, symmetry_axes="2" (axisymmetric; the 72x12x2 workload)
   sph3d  : Spherical, full 3-D (batched and adjoint workloads)
   sinh3d : SinhSpherical, full 3-D (the 256x64x64 workloads)
+  sph3dck: sph3d plus write_checkpoint/read_checkpoint (checkpoint file parity)
 
 Usage: python oracle/gen_ref.py [--variants sphaxi,sph3d,sinh3d] [--reference DIR]
 """
@@ -38,7 +39,10 @@ VARIANTS = {
     "sphaxi": ["--coord", "Spherical", "--axisym"],
     "sph3d": ["--coord", "Spherical"],
     "sinh3d": ["--coord", "SinhSpherical"],
+    "sph3dck": ["--coord", "Spherical", "--checkpoint"],
 }
+# Extra compiler definitions of a variant's harness build.
+HARNESS_DEFS = {"sph3dck": ["-DREF_HAS_CHECKPOINT"]}
 ISAS = {"avx512": "-march=x86-64-v4", "avx2": "-march=x86-64-v3"}
 
 
@@ -81,7 +85,7 @@ def compile_variant(variant: str, proj: pathlib.Path, jobs: int) -> None:
     for isa, march in ISAS.items():
         objdir = vdir / f"obj_{isa}"
         objdir.mkdir(exist_ok=True)
-        base = ["gcc", "-std=gnu99", "-O2", march, "-fopenmp", "-fPIC", "-w", f"-I{proj}"]
+        base = ["gcc", "-std=gnu99", "-O2", march, "-fopenmp", "-fPIC", "-w", f"-I{proj}"] + HARNESS_DEFS.get(variant, [])
 
         def one(src: pathlib.Path) -> pathlib.Path:
             rel = src.relative_to(proj) if proj in src.parents else pathlib.Path(src.name)

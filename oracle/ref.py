@@ -83,6 +83,19 @@ def _load(variant: str) -> C.CDLL:
     lib.ref_dV.argtypes = [vp, ip, ip, ip]
     lib.ref_diagnostics.argtypes = [vp, ip, C.c_double, C.c_double]
     lib.ref_initial_data.argtypes = [vp]
+    lib.ref_set_clock.argtypes = [vp, ip, C.c_double]
+    lib.ref_commondata.restype = vp
+    lib.ref_commondata.argtypes = [vp]
+    lib.ref_t_0.restype = C.c_double
+    lib.ref_t_0.argtypes = [vp]
+    lib.ref_nn_0.argtypes = [vp]
+    if hasattr(lib, "ref_write_checkpoint"):
+        lib.ref_write_checkpoint.argtypes = [vp, C.c_double]
+        lib.ref_read_checkpoint.argtypes = [vp]
+        lib.ref_checkpoint_every.restype = C.c_double
+        lib.ref_checkpoint_every.argtypes = [vp]
+        lib.ref_offsetof_commondata_checkpoint_every.restype = C.c_size_t
+        lib.ref_offsetof_commondata_checkpoint_every.argtypes = []
     lib.ref_destroy.argtypes = [vp]
     for f in ("ref_sizeof_commondata", "ref_sizeof_params", "ref_sizeof_bc_struct", "ref_sizeof_griddata",
               "ref_sizeof_innerpt", "ref_sizeof_outerpt", "ref_offsetof_params_Nxx0", "ref_offsetof_params_invdxx0",
@@ -193,6 +206,33 @@ class RefGrid:
     def diagnostics(self, nn: int, time: float, output_every: float) -> None:
         """The generated diagnostics() driver at the present state (files in the current directory)."""
         self.lib.ref_diagnostics(self.h, int(nn), float(time), float(output_every))
+
+    def commondata_bytes(self) -> bytes:
+        """The raw bytes of the project's commondata_struct."""
+        return C.string_at(self.lib.ref_commondata(self.h), self.lib.ref_sizeof_commondata())
+
+    def set_clock(self, nn: int, time: float) -> None:
+        self.lib.ref_set_clock(self.h, int(nn), float(time))
+
+    def nn(self) -> int:
+        return self.lib.ref_nn(self.h)
+
+    def t_0(self) -> float:
+        return self.lib.ref_t_0(self.h)
+
+    def nn_0(self) -> int:
+        return self.lib.ref_nn_0(self.h)
+
+    def write_checkpoint(self, checkpoint_every: float) -> None:
+        """The generated write_checkpoint() (checkpoint-enabled variant; current directory)."""
+        self.lib.ref_write_checkpoint(self.h, float(checkpoint_every))
+
+    def read_checkpoint(self) -> int:
+        """The generated read_checkpoint(): 0 without a file, 1 after restoring commondata and y_n."""
+        return self.lib.ref_read_checkpoint(self.h)
+
+    def checkpoint_every(self) -> float:
+        return self.lib.ref_checkpoint_every(self.h)
 
     def dV(self) -> np.ndarray:
         G = NGHOSTS

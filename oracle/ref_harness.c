@@ -197,3 +197,21 @@ void ref_diagnostics(ref_sim *s, int nn, double time, double output_every) {
 }
 // The generated initial_data() (Brill-Lindquist -> BSSN, lambda^i, BCs) on this grid.
 void ref_initial_data(ref_sim *s) { initial_data(&s->commondata, s->griddata); }
+// Clock of the run (the test sets the same step counter and time on both sides).
+void ref_set_clock(ref_sim *s, int nn, double time) {
+  s->commondata.nn = nn;
+  s->commondata.time = time;
+}
+double ref_t_0(ref_sim *s) { return s->commondata.t_0; }
+int ref_nn_0(ref_sim *s) { return s->commondata.nn_0; }
+#ifdef REF_HAS_CHECKPOINT
+// The generated write_checkpoint()/read_checkpoint() (checkpointing.py:15-470) of a project that
+// registers checkpointing; the file checkpoint-conv_factor%.2f.dat is in the current directory.
+void ref_write_checkpoint(ref_sim *s, double checkpoint_every) {
+  s->commondata.checkpoint_every = checkpoint_every;
+  write_checkpoint(&s->commondata, s->griddata);
+}
+int ref_read_checkpoint(ref_sim *s) { return read_checkpoint(&s->commondata, s->griddata); }
+double ref_checkpoint_every(ref_sim *s) { return s->commondata.checkpoint_every; }
+size_t ref_offsetof_commondata_checkpoint_every(void) { return offsetof(commondata_struct, checkpoint_every); }
+#endif

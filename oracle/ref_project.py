@@ -10,7 +10,9 @@ nrpy/examples/two_blackholes_collide.py:60-440 with the settings the workloads n
   (two_blackholes_collide.py:141-143), otherwise the grid is full 3-D;
 * the BHaHAHA horizon finder off (it is a diagnostic, not the step);
 * every coordinate system's CodeParameters registered ("All"), so that one
-  params_struct layout serves every project variant.
+  params_struct layout serves every project variant;
+* ``--checkpoint`` also registers write_checkpoint/read_checkpoint (checkpointing.py:473-490),
+  which adds the REAL CodeParameter checkpoint_every to commondata_struct.
 
 Run it with the reference on PYTHONPATH (oracle/gen_ref.py does this).
 """
@@ -30,6 +32,7 @@ ap.add_argument("--coord", default="Spherical")
 ap.add_argument("--axisym", action="store_true")
 ap.add_argument("--project-dir", required=True)
 ap.add_argument("--cuda", action="store_true")
+ap.add_argument("--checkpoint", action="store_true")
 args = ap.parse_args()
 
 parallelization = "cuda" if args.cuda else "openmp"
@@ -161,6 +164,10 @@ BHaH.MoLtimestepping.register_all.register_CFunctions(
 BHaH.xx_tofrom_Cart.register_CFunction_Cart_to_xx_and_nearest_i0i1i2_assume_valid(CoordSystem)
 BHaH.xx_tofrom_Cart.register_CFunction_xx_to_Cart(CoordSystem)
 BHaH.diagnostics.progress_indicator.register_CFunction_progress_indicator()
+if args.checkpoint:
+    import nrpy.infrastructures.BHaH.checkpointing as checkpointing
+
+    checkpointing.register_CFunctions(default_checkpoint_every=2.0)
 BHaH.general_relativity.basis_transforms.register_all.register_CFunctions(
     set_of_CoordSystems=set_of_CoordSystems
 )
