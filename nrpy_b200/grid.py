@@ -260,27 +260,35 @@ class BSSNGrid:
             L.check(self.lib.bssn_b200_mol_step(C.byref(self.cd), self.gd, mode, int(mixed), self.stream))
 
     def step_from_host(self, host_in: Sequence[torch.Tensor], host_out: Sequence[torch.Tensor], mode: int = 1,
-                       mixed: bool = False, on_step=None) -> None:
+                       mixed: bool = False, on_step=None, graph: bool = True) -> None:
         """One RK4 step for each host state: host_in[i] (pinned, NUM_EVOL_GFS gridfunctions)
         -> device -> one step -> host_out[i].
 
         The copies overlap the steps: the state alternates between two device buffers, the
         upload of state i+1 runs on its own stream during step i and the download of state i
-        on a third stream during step i+1. Steps run in order on the current stream (they share
-        the grid's stage buffers). ``on_step(i, y)`` (optional) is called on the current stream
-        after step i with the device state. y_n_gfs points at this grid's own y_n again on return."""
+        on a third stream during step i+1. Steps run in order on a compute stream that follows
+        the current stream (they share the grid's stage buffers). With ``graph`` each step is a
+        replay of a CUDA graph of one RK4 step captured for that device buffer (two graphs, kept
+        until dt, mode or mixed change); otherwise each step's kernels are launched one by one.
+        ``on_step(i, y)`` (optional) is called with the compute stream current after step i
+        with the device state. y_n_gfs points at this grid's own y_n again on return."""
         n = len(host_in)
         if len(host_out) != n:
             raise ValueError("host_in and host_out must have the same length")
         if getattr(self, "_y_alt", None) is None:
             self._y_alt = torch.empty_like(self.y_n)
         dev = [self.y_n, self._y_alt]
-        comp = torch.cuda.current_stream(self.device)
+        caller = torch.cuda.current_stream(self.device)
+        if getattr(self, "_host_comp", None) is None:
+            self._host_comp = torch.cuda.Stream(self.device)
+        comp = self._host_comp
+        comp.wait_stream(caller)
         h2d, d2h = torch.cuda.Stream(self.device), torch.cuda.Stream(self.device)
         h2d.wait_stream(comp)
         d2h.wait_stream(comp)
         freed = [None, None]  # event: the last download from buffer k has finished
         gf = self.gd[0].gridfuncs
+        graphs = self._host_graphs_for(dev, mode, mixed, comp) if graph else None
         try:
             for i in range(n):
                 k = i % 2
@@ -291,11 +299,15 @@ class BSSNGrid:
                     loaded = torch.cuda.Event()
                     loaded.record(h2d)
                 comp.wait_event(loaded)
-                gf.y_n_gfs = _ptr(dev[k])
-                L.check(self.lib.bssn_b200_mol_step(C.byref(self.cd), self.gd, mode, int(mixed),
-                                                    C.c_void_p(comp.cuda_stream)))
+                if graphs is not None:
+                    L.check(self.lib.bssn_b200_stepper_run(graphs[k], 1))
+                else:
+                    gf.y_n_gfs = _ptr(dev[k])
+                    L.check(self.lib.bssn_b200_mol_step(C.byref(self.cd), self.gd, mode, int(mixed),
+                                                        C.c_void_p(comp.cuda_stream)))
                 if on_step is not None:
-                    on_step(i, dev[k])
+                    with torch.cuda.stream(comp):
+                        on_step(i, dev[k])
                 stepped = torch.cuda.Event()
                 stepped.record(comp)
                 with torch.cuda.stream(d2h):
@@ -308,6 +320,39 @@ class BSSNGrid:
             gf.y_n_gfs = _ptr(self.y_n)
             comp.wait_stream(h2d)
             comp.wait_stream(d2h)
+            caller.wait_stream(comp)
+
+    def _host_graphs_for(self, dev, mode: int, mixed: bool, comp):
+        """The two one-step graphs of step_from_host (device buffer 0 and 1), captured on comp."""
+        key = (int(mode), bool(mixed), comp.cuda_stream, float(self.cd.dt), dev[0].data_ptr(), dev[1].data_ptr())
+        cached = getattr(self, "_host_graphs", None)
+        if cached is not None and cached[0] == key:
+            return cached[1]
+        self._free_host_graphs()
+        gf = self.gd[0].gridfuncs
+        sts = []
+        try:
+            for k in (0, 1):
+                gf.y_n_gfs = _ptr(dev[k])
+                st = C.c_void_p()
+                L.check(self.lib.bssn_b200_stepper_create(C.byref(self.cd), self.gd, int(mode), int(mixed), 1,
+                                                          C.c_void_p(comp.cuda_stream), C.byref(st)))
+                sts.append(st)
+        except Exception:
+            for st in sts:
+                self.lib.bssn_b200_stepper_destroy(st)
+            raise
+        finally:
+            gf.y_n_gfs = _ptr(self.y_n)
+        self._host_graphs = (key, sts)
+        return sts
+
+    def _free_host_graphs(self) -> None:
+        cached = getattr(self, "_host_graphs", None)
+        if cached is not None:
+            for st in cached[1]:
+                self.lib.bssn_b200_stepper_destroy(st)
+            self._host_graphs = None
 
     def make_stepper(self, mode: int = 1, mixed: bool = False, steps_per_graph: int = 1, stream=None):
         """Capture `steps_per_graph` RK4 steps into a CUDA graph bound to this grid's buffers."""
@@ -327,9 +372,11 @@ class BSSNGrid:
         L.check(self.lib.bssn_b200_stepper_run(self._stepper, graph_launches))
 
     def free_stepper(self) -> None:
+        """Release the captured graphs (make_stepper's and step_from_host's)."""
         if getattr(self, "_stepper", None) is not None:
             self.lib.bssn_b200_stepper_destroy(self._stepper)
             self._stepper = None
+        self._free_host_graphs()
 
     def close(self) -> None:
         self.free_stepper()
