@@ -409,7 +409,9 @@ int bssn_b200_diagnostics(commondata_struct *commondata, griddata_struct *gridda
  * (checkpointing.py:253-255); the generated struct lists REAL fields by name, which puts it after
  * KreissOliger_strength_nongauge. This library's commondata_struct is the layout of a project
  * without it, so the cadence is an argument here and no drop-in named write_checkpoint or
- * read_checkpoint is exported (its commondata argument would have the other layout). */
+ * read_checkpoint is exported (its commondata argument would have the other layout).
+ * The first call on a device allocates staging buffers (two 12.6 MB device chunks and two 12.6 MB
+ * pinned host chunks) that the library keeps until the process exits; calls are serialised. */
 typedef struct {
   REAL BH1_mass;
   REAL BH1_posn_x;

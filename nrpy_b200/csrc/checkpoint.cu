@@ -15,6 +15,7 @@
 #include <cerrno>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "bssn_common.cuh"
@@ -62,8 +63,39 @@ __global__ void __launch_bounds__(CK_THREADS) scatter_points_kernel(const double
   }
 }
 
-// Device and pinned buffers of one call, released on every return path.
+// Staging buffers of one device: two device chunks, two pinned host chunks and their events.
+// Allocated on the first checkpoint call on that device and kept until the process exits
+// (2 x 12.6 MB of device memory and 2 x 12.6 MB of pinned host memory), so repeated checkpoints
+// pay no allocation. Calls are serialised by the mutex.
+struct Staging {
+  double *dev[2] = {nullptr, nullptr};
+  double *host[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+};
+std::mutex g_staging_mu;
+Staging g_staging[64];
+
+int staging_for_current_device(Staging **out) {
+  int d = 0;
+  BSSN_CUDA_TRY(cudaGetDevice(&d));
+  if (d < 0 || d >= 64) {
+    set_error("checkpoint: device ordinal %d not supported", d);
+    return BSSN_B200_EINVAL;
+  }
+  Staging &st = g_staging[d];
+  for (int b = 0; b < 2; b++) {
+    if (!st.dev[b]) BSSN_CUDA_TRY(cudaMalloc(&st.dev[b], CK_CHUNK * NUM_EVOL_GFS * sizeof(double)));
+    if (!st.host[b]) BSSN_CUDA_TRY(cudaMallocHost(&st.host[b], CK_CHUNK * NUM_EVOL_GFS * sizeof(double)));
+    if (!st.ev[b]) BSSN_CUDA_TRY(cudaEventCreateWithFlags(&st.ev[b], cudaEventDisableTiming));
+  }
+  *out = &st;
+  return BSSN_B200_OK;
+}
+
+// One call's view of the staging buffers, plus what it owns itself (the file, the device copy
+// of the read indices); on every return path it waits for its copies and closes the file.
 struct Pipeline {
+  std::lock_guard<std::mutex> lock{g_staging_mu};
   double *dev[2] = {nullptr, nullptr};
   double *host[2] = {nullptr, nullptr};
   int *dev_idx = nullptr;
@@ -73,19 +105,16 @@ struct Pipeline {
     for (int b = 0; b < 2; b++) {
       if (ev[b]) cudaEventSynchronize(ev[b]);
     }
-    for (int b = 0; b < 2; b++) {
-      if (dev[b]) cudaFree(dev[b]);
-      if (host[b]) cudaFreeHost(host[b]);
-      if (ev[b]) cudaEventDestroy(ev[b]);
-    }
     if (dev_idx) cudaFree(dev_idx);
     if (f) fclose(f);
   }
-  int alloc(size_t points) {
+  int attach() {
+    Staging *st = nullptr;
+    BSSN_TRY(staging_for_current_device(&st));
     for (int b = 0; b < 2; b++) {
-      BSSN_CUDA_TRY(cudaMalloc(&dev[b], points * NUM_EVOL_GFS * sizeof(double)));
-      BSSN_CUDA_TRY(cudaMallocHost(&host[b], points * NUM_EVOL_GFS * sizeof(double)));
-      BSSN_CUDA_TRY(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+      dev[b] = st->dev[b];
+      host[b] = st->host[b];
+      ev[b] = st->ev[b];
     }
     return BSSN_B200_OK;
   }
@@ -238,9 +267,7 @@ int write_checkpoint_impl(const commondata_struct *cd, const double checkpoint_e
   char fname[256];
   checkpoint_filename(cd->convergence_factor, fname);
   Pipeline pl;
-  size_t maxpts = 0;
-  for (int grid = 0; grid < cd->NUMGRIDS; grid++) maxpts = std::max(maxpts, grid_points(gd[grid].params));
-  BSSN_TRY(pl.alloc(std::min(CK_CHUNK, std::max<size_t>(maxpts, 1))));
+  BSSN_TRY(pl.attach());
   pl.f = fopen(fname, "wb");
   if (!pl.f) {
     set_error("write_checkpoint: could not open %s for writing: %s", fname, strerror(errno));
@@ -327,9 +354,7 @@ int read_checkpoint_impl(commondata_struct *cd, double *checkpoint_every, gridda
     return 1;
   }
   BSSN_TRY(check_numgrids(ck.NUMGRIDS, "read_checkpoint"));
-  size_t maxpts = 1;
-  for (int grid = 0; grid < ck.NUMGRIDS; grid++) maxpts = std::max(maxpts, grid_points(gd[grid].params));
-  BSSN_TRY(pl.alloc(std::min(CK_CHUNK, maxpts)));
+  BSSN_TRY(pl.attach());
   for (int grid = 0; grid < ck.NUMGRIDS; grid++) {
     griddata_struct &g = gd[grid];
     params_struct saved;
