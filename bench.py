@@ -307,7 +307,7 @@ def main():
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
                          "traffic": profiled_traffic() if NXX == (256, 64, 64) else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the three group "
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the two rhs group "
                                            "launches of one stage at 256x64x32, scaled by point count",
                          "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": kstats["ms_per_launch"],
                          "step_achieved": value / world * B_ALG_PER_PT_STEP / 1e9,
