@@ -130,8 +130,11 @@ class _Printer(C99CodePrinter):
 class PointKernel:
     """Collects leaf definitions and CSE'd statements for one pointwise function."""
 
-    def __init__(self, symmetry_axes: str = ""):
+    def __init__(self, symmetry_axes: str = "", leaf_index: Optional[Dict[str, int]] = None):
         self.sym_axes = {int(c) for c in symmetry_axes}
+        # With a leaf index, finite-difference leaves are read from a precomputed leaf array
+        # (LDLEAF(k)) instead of being evaluated from stencil loads.
+        self.leaf_index = leaf_index
         self.lines: List[str] = []
         self.defined: Set[str] = set()
         self.loaded: Set[Tuple[str, Tuple[int, int, int]]] = set()
@@ -183,6 +186,9 @@ class PointKernel:
             raise KeyError(f"unknown symbol {name}")
         gf, kind, dirs = pd
         self.stats["derivs"] += 1
+        if self.leaf_index is not None:
+            self.lines.append(f"const T {name} = T(LDLEAF({self.leaf_index[name]}));")
+            return
         self.lines.append(self._deriv_code(name, gf, kind, dirs))
 
     def _deriv_code(self, name: str, gf: str, kind: str, dirs: Tuple[int, ...]) -> str:
@@ -241,7 +247,7 @@ class PointKernel:
         for s in sorted(expr.free_symbols, key=lambda x: x.name):
             if s.name.startswith("_"):
                 continue
-            if parse_deriv(s.name) and parse_deriv(s.name)[1] == "upD":
+            if parse_deriv(s.name) and parse_deriv(s.name)[1] == "upD" and self.leaf_index is None:
                 self._ensure_upwind()
             self._define_leaf(s.name)
 
@@ -426,7 +432,8 @@ def _parse(lines: List[str]):
 def _is_remat(ty: str, rhs: str, remat: Dict[str, str], deriv_remat: bool = False) -> bool:
     if ty == "double" and rhs.startswith("LD("):
         return True
-    if ty == "T" and (rhs.startswith("T(RFM(") or rhs.startswith("T(PARAM(") or rhs.startswith("T(LDAUX(")):
+    if ty == "T" and (rhs.startswith("T(RFM(") or rhs.startswith("T(PARAM(") or rhs.startswith("T(LDAUX(")
+                      or rhs.startswith("T(LDLEAF(")):
         return True
     if deriv_remat and ty == "T" and rhs.startswith("T(TF(invdxx"):
         return True  # finite difference: recomputed from its stencil loads at each use
@@ -542,12 +549,13 @@ def emit_point_function(
     remat_first: bool = False,
     deriv_remat: bool = False,
     order: str = "dfs",
+    leaf_index: Optional[Dict[str, int]] = None,
 ) -> Tuple[str, Dict[str, int]]:
     """Emit `fname` and the constant `fname_SMEM_SLOTS`. With reg_capacity > 0 the values
     beyond that many live doubles go to shared-memory slots (SMEM(k), provided by the
     caller through the `sm` argument: slot k of this thread; the template parameter NT is
     the slot stride, i.e. the threads of a block)."""
-    pk = PointKernel(symmetry_axes)
+    pk = PointKernel(symmetry_axes, leaf_index)
     pk.build(outputs, upwind_vec)
     if reg_capacity > 0:
         # Statement order: "dfs" completes one output at a time (dfs_order); "sched" keeps the
@@ -568,3 +576,35 @@ def emit_point_function(
     stats = dict(pk.stats)
     stats["smem_slots"] = nslots
     return code, stats
+
+
+def leaf_names(exprs: Sequence[sp.Expr]) -> List[str]:
+    """Finite-difference leaves of a set of expressions, grouped by gridfunction (sorted)."""
+    names = set()
+    for e in exprs:
+        for x in sp.sympify(e).free_symbols:
+            if parse_deriv(x.name):
+                names.add(x.name)
+    return sorted(names, key=lambda n: (parse_deriv(n)[0], n))
+
+
+def emit_leaf_function(fname: str, names: Sequence[str], upwind_vec=None, symmetry_axes: str = "",
+                       comment: str = "") -> Tuple[str, Dict[str, int]]:
+    """Emit `fname`, which evaluates the finite-difference leaves `names` at one point from
+    stencil loads (the same statements the point functions use) and stores leaf k through
+    LEAFOUT(k, value). The upwinded leaves use the point's shift vector (upwind_vec)."""
+    pk = PointKernel(symmetry_axes)
+    pk.upwind_vec = upwind_vec
+    for k, name in enumerate(names):
+        if parse_deriv(name)[1] == "upD":
+            pk._ensure_upwind()
+        pk._define_leaf(name)
+        pk.lines.append(f"LEAFOUT({k}, {name});")
+    body = "\n".join("  " + ln for ln in pk.lines)
+    head = f"// {comment}\n" if comment else ""
+    code = (
+        f"{head}constexpr int {fname}_NUM_LEAVES = {len(names)};\n"
+        f"template <typename T, typename TF, typename Ctx>\n"
+        f"__device__ __forceinline__ void {fname}(const Ctx &ctx) {{\n{body}\n}}\n"
+    )
+    return code, dict(pk.stats)

@@ -6,6 +6,7 @@ flags in generate.py come from its measurements). Three steps:
   python -m nrpy_b200.codegen.tune_groups generate   # needs nrpy (equation modules)
   python -m nrpy_b200.codegen.tune_groups generate-orders  # present groups x statement orders
   python -m nrpy_b200.codegen.tune_groups generate-caps    # present groups x register budgets
+  python -m nrpy_b200.codegen.tune_groups generate-leaf    # present groups on precomputed FD leaves
   python -m nrpy_b200.codegen.tune_groups compile    # nvcc, sm_100a, no GPU needed
   python -m nrpy_b200.codegen.tune_groups run        # on a B200; prints one line per kernel
 
@@ -256,6 +257,73 @@ def generate_caps(caps) -> None:
         print(tag, flush=True)
 
 
+LEAF_CAPS = (64, 72, 90, 120, 160)
+
+
+def generate_leaf() -> None:
+    """The present groups reading precomputed finite-difference leaves (one array per leaf,
+    LDLEAF) at several register budgets, beside their stencil form, and the kernel that
+    computes every leaf from stencils (LEAFOUT): is precomputing the derivatives cheaper
+    than evaluating them in each group?"""
+    from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen.emit_cuda import emit_leaf_function, emit_point_function, leaf_names
+    from nrpy_b200.codegen.generate import RHS_ALLOC, RHS_CAPS, RICCI_ALLOC, RICCI_CAPS
+
+    be.setup_nrpy("")
+    rhs, betaU = be.rhs_exprs("SinhSpherical")
+    ricci = be.ricci_exprs("SinhSpherical")
+    names = leaf_names(list(rhs.values()) + list(ricci.values()))
+    index = {n: k for k, n in enumerate(names)}
+    OUT.mkdir(parents=True, exist_ok=True)
+    head = HARNESS_HEAD
+    for a, b in (
+        ("double eta, KreissOliger_strength_gauge, KreissOliger_strength_nongauge;",
+         "double eta, KreissOliger_strength_gauge, KreissOliger_strength_nongauge; const double *__restrict__ leaf; "
+         "double *leafout;"),
+        ("#define LDAUX(k) ctx.ldaux(k)", "#define LDAUX(k) ctx.ldaux(k)\n#define LDLEAF(k) __ldg(ctx.leaf + (size_t)(k) * NTOT)"
+         "\n#define LEAFOUT(k, v) ctx.leafout[(size_t)(k) * NTOT] = (v)"),
+        ("constexpr int N0 = 262, N1 = 70, N2 = 38, NTOT = N0 * N1 * N2, MAXOUT = 18;\n", ""),
+        ('#include "GROUP.cuh"', 'constexpr int N0 = 262, N1 = 70, N2 = 38, NTOT = N0 * N1 * N2, MAXOUT = 18;\n'
+         '#include "GROUP.cuh"'),
+        ("ctx.KreissOliger_strength_nongauge = 0.3;",
+         "ctx.KreissOliger_strength_nongauge = 0.3; ctx.leaf = g_leaf + idx; ctx.leafout = g_leaf + idx;"),
+        ("template <int NT, int MINB, int NOUT, class F>\n__global__",
+         "__device__ double *g_leaf;\ntemplate <int NT, int MINB, int NOUT, class F>\n__global__"),
+    ):
+        assert a in head
+        head = head.replace(a, b, 1)
+    parts, wrappers, calls = ["#pragma once\n"], [], []
+    parts.append(emit_leaf_function("leaf_all", names, upwind_vec=betaU)[0])
+    chosen = dict(zip(ORDER_GROUPS, zip(list(RICCI_ALLOC) + list(RHS_ALLOC), list(RICCI_CAPS) + list(RHS_CAPS))))
+    for gname in ORDER_GROUPS:
+        kind, gn = CANDIDATES[gname]
+        src, uv = (ricci, None) if kind == "ricci" else (rhs, betaU)
+        (rf, dr, order), cap0 = chosen[gname]
+        for tag, cap, li in [("stencil", cap0, None)] + [(f"leaf{c}", c, index) for c in LEAF_CAPS]:
+            fname = f"{gname}_{tag}"
+            code, st = emit_point_function(fname, [(f"out[{i}]", src[n]) for i, n in enumerate(gn)], upwind_vec=uv,
+                                           reg_capacity=cap, remat_first=rf, deriv_remat=dr, order=order, leaf_index=li)
+            parts.append(code)
+            slots = max(st["smem_slots"], 1)
+            wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
+                            f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
+            nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
+            calls.append(f'  run<{nt}, 1, {len(gn)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+    wrappers.append("struct W_leaf { template <int NT, class C> __device__ __forceinline__ static void "
+                    "eval(const C &c, double *o, volatile double *sm) { leaf_all<double, double>(c); o[0] = 0.0; } };")
+    calls.append('  run<128, 1, 1, 1, W_leaf>("leaf_all", rfm, in, aux, out);')
+    (OUT / "leaf.cuh").write_text("\n".join(parts))
+    h, m = head.replace("GROUP", "leaf").split("int main() {")
+    n = len(names)
+    m = m.replace("RfmArrays rfm{",
+                  f"double *lb; cudaMalloc(&lb, (size_t)NTOT * {n} * 8);\n"
+                  f"  for (int k = 0; k < {n}; k++) cudaMemcpy(lb + (size_t)k * NTOT, in + (size_t)(k % 24) * NTOT, "
+                  "(size_t)NTOT * 8, cudaMemcpyDeviceToDevice);\n"
+                  "  cudaMemcpyToSymbol(g_leaf, &lb, sizeof(lb));\n  RfmArrays rfm{", 1)
+    (OUT / "leaf.cu").write_text(h + "\n".join(wrappers) + "\nint main() {" + m + "\n".join(calls) + "\n  return 0;\n}\n")
+    print(f"leaf: {n} leaves", flush=True)
+
+
 def compile_all(jobs: int) -> None:
     from nrpy_b200.build import nvcc
 
@@ -294,7 +362,8 @@ def summarize(path: str) -> None:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["generate", "generate-orders", "generate-caps", "compile", "run", "summarize"])
+    ap.add_argument("step", choices=["generate", "generate-orders", "generate-caps", "generate-leaf", "compile", "run",
+                                     "summarize"])
     ap.add_argument("--caps", default="72,80,90,100")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--log", default=None)
@@ -305,6 +374,8 @@ if __name__ == "__main__":
         generate_orders()
     elif a.step == "generate-caps":
         generate_caps([int(c) for c in a.caps.split(",")])
+    elif a.step == "generate-leaf":
+        generate_leaf()
     elif a.step == "compile":
         compile_all(a.jobs)
     elif a.step == "run":
