@@ -34,7 +34,14 @@ extern "C" {
 #ifndef REAL
 #define REAL double
 #endif
-#define NGHOSTS 3
+/* Interior finite-difference order of this build: 4 (libbssn_b200.so, the default) or 8
+ * (libbssn_b200_fd8.so, built with -DBSSN_B200_FD_ORDER=8). NGHOSTS = order/2 + 1, as the
+ * generated project's BHaH_defines.h sets it for fd_order with upwinding/KO, so the structs
+ * below that depend on it (bc_info_struct, bc_struct) match a project of the same order. */
+#ifndef BSSN_B200_FD_ORDER
+#define BSSN_B200_FD_ORDER 4
+#endif
+#define NGHOSTS (BSSN_B200_FD_ORDER / 2 + 1)
 #define NUM_EVOL_GFS 24
 #define NUM_AUXEVOL_GFS 6
 #define MAXNUMGRIDS 15
@@ -287,6 +294,8 @@ enum {
 };
 const char *bssn_b200_last_error(void);
 const char *bssn_b200_version(void);
+/* BSSN_B200_FD_ORDER of the loaded library (4 or 8). */
+int bssn_b200_fd_order(void);
 
 /* Symmetry axes of the generated algebra: "" (full 3-D, default) or "2" (axisymmetric:
  * derivatives in xx2 vanish, as nrpy's symmetry_axes="2"). Process-wide setting. */

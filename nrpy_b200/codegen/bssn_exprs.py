@@ -29,14 +29,14 @@ GF_ORDER = [
 RBAR_ORDER = ["RbarDD00", "RbarDD01", "RbarDD02", "RbarDD11", "RbarDD12", "RbarDD22"]
 
 
-def setup_nrpy(symmetry_axes: str) -> None:
+def setup_nrpy(symmetry_axes: str, fd_order: int = 4) -> None:
     import nrpy.finite_difference  # noqa: F401  (registers fd_order)
     import nrpy.indexedexp  # noqa: F401  (registers symmetry_axes)
     import nrpy.params as par
 
     par.set_parval_from_str("Infrastructure", "BHaH")
     par.set_parval_from_str("fp_type", "double")
-    par.set_parval_from_str("fd_order", 4)
+    par.set_parval_from_str("fd_order", fd_order)
     par.set_parval_from_str("symmetry_axes", symmetry_axes)
 
 

@@ -1,6 +1,9 @@
-"""Finite-difference weights for the 4th-order BHaH stencils, derived from Taylor series.
+"""Finite-difference weights of the BHaH stencils (4th order by default), derived from Taylor series.
 
 The operator set and stencil placement follow nrpy/finite_difference.py:202-330:
+
+Offsets below are for the default 4th order; ``set_fd_order`` selects another even order
+(radius order/2, KO derivative of order order+2 on order+3 points).
 
 * ``dD``   first derivative, centred, offsets -2..2;
 * ``dDD``  second derivative, centred (unmixed) or the product of two centred first
@@ -22,6 +25,18 @@ import sympy as sp
 
 FD_ORDER = 4
 NGHOSTS = 3
+# The outer radiation condition keeps its own 4th-order one-sided derivatives whatever the
+# interior order (radiation_BC_fd_order = 4 in the generated projects).
+RADIATION_BC_FD_ORDER = 4
+
+
+def set_fd_order(order: int) -> None:
+    """Interior finite-difference order (even); NGHOSTS = order/2 + 1 (one more for the
+    upwinded stencils and KO dissipation)."""
+    global FD_ORDER, NGHOSTS
+    if order < 2 or order % 2:
+        raise ValueError(f"fd_order {order}: an even order >= 2")
+    FD_ORDER, NGHOSTS = order, order // 2 + 1
 
 
 @lru_cache(maxsize=None)
@@ -69,6 +84,6 @@ def radiation_fd1(offset: int) -> Dict[int, sp.Rational]:
     nrpy/infrastructures/BHaH/CurviBoundaryConditions/apply_bcs_outerradiation_and_inner.py:122-278
     for radiation_BC_fd_order = 4 (offset in -2..2).
     """
-    offs = tuple(s + offset for s in centred_offsets(FD_ORDER // 2))
+    offs = tuple(s + offset for s in centred_offsets(RADIATION_BC_FD_ORDER // 2))
     w = weights(offs, 1)
     return {s: c for s, c in zip(offs, w) if c != 0}

@@ -5,7 +5,7 @@ PYTHONPATH. The emitted headers are committed, so building the CUDA library does
 need nrpy. Each (CoordSystem, symmetry) variant is generated in its own process because
 nrpy caches equation objects per CoordSystem and reads ``symmetry_axes`` globally.
 
-Usage: python -m nrpy_b200.codegen.generate [--reference PATH] [--variants ...]
+Usage: python -m nrpy_b200.codegen.generate [--reference PATH] [--variants ...] [--fd-order N --adjoint ""]
 """
 
 import argparse
@@ -96,12 +96,19 @@ def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int) -> s
     )
 
 
-def generate_variant(tag: str) -> None:
+def header_name(tag: str, fd_order: int) -> str:
+    """Generated header of a variant: bssn_<tag>.cuh (4th order) or bssn_<tag>_fd<order>.cuh."""
+    return f"bssn_{tag}.cuh" if fd_order == 4 else f"bssn_{tag}_fd{fd_order}.cuh"
+
+
+def generate_variant(tag: str, fd_order: int = 4) -> None:
     from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen import fdcoeffs as fdc
     from nrpy_b200.codegen.emit_cuda import emit_point_function
 
     coord, sym = VARIANTS[tag]
-    be.setup_nrpy(sym)
+    fdc.set_fd_order(fd_order)
+    be.setup_nrpy(sym, fd_order)
     t0 = time.time()
     rhs, betaU = be.rhs_exprs(coord)
     ricci = be.ricci_exprs(coord)
@@ -167,15 +174,15 @@ def generate_variant(tag: str) -> None:
                    f"constexpr int rhs_group_count_{tag} = {len(RHS_GROUPS)};\n")
     hdr = (
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
-        f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', 4th-order FD, KO (CAKO).\n"
+        f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', {fd_order}th-order FD, KO (CAKO).\n"
         f"// Register budgets Ricci {RICCI_CAPS}, RHS {RHS_CAPS} values; allocation (remat_first, deriv_remat, "
         f"order): Ricci {RICCI_ALLOC}, RHS {RHS_ALLOC}.\n"
         f"// Per point: {stats}\n"
         "#pragma once\n\n"
     )
     OUTDIR.mkdir(parents=True, exist_ok=True)
-    (OUTDIR / f"bssn_{tag}.cuh").write_text(hdr + "\n".join(parts) + "\n" + "\n".join(structs))
-    print(f"{tag}: {stats} ({time.time() - t0:.1f}s)")
+    (OUTDIR / header_name(tag, fd_order)).write_text(hdr + "\n".join(parts) + "\n" + "\n".join(structs))
+    print(f"{tag} (fd_order {fd_order}): {stats} ({time.time() - t0:.1f}s)")
 
 
 def _c_rational(r) -> str:
@@ -307,11 +314,13 @@ def main() -> None:
     ap.add_argument("--reference", default="/root/reference")
     ap.add_argument("--variants", default=",".join(VARIANTS))
     ap.add_argument("--adjoint", default=",".join(ADJOINT_VARIANTS))
+    ap.add_argument("--fd-order", type=int, default=4,
+                    help="interior FD order of the forward variants (the adjoint is 4th order only)")
     ap.add_argument("--one", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--one-adjoint", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.one:
-        generate_variant(args.one)
+        generate_variant(args.one, args.fd_order)
         return
     if args.one_adjoint:
         generate_adjoint(args.one_adjoint)
@@ -320,9 +329,12 @@ def main() -> None:
     env = dict(os.environ)
     env["PYTHONPATH"] = f"{ROOT}:{shim}:{args.reference}"
     procs = [
-        subprocess.Popen([sys.executable, "-m", "nrpy_b200.codegen.generate", "--one", tag], env=env, cwd=ROOT)
+        subprocess.Popen([sys.executable, "-m", "nrpy_b200.codegen.generate", "--one", tag, "--fd-order",
+                          str(args.fd_order)], env=env, cwd=ROOT)
         for tag in args.variants.split(",") if tag
     ]
+    if args.fd_order != 4 and args.adjoint:
+        raise SystemExit("the adjoint variants are 4th order only: pass --adjoint ''")
     procs += [
         subprocess.Popen([sys.executable, "-m", "nrpy_b200.codegen.generate", "--one-adjoint", tag], env=env,
                          cwd=ROOT)

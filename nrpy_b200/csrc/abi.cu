@@ -121,6 +121,8 @@ const REAL gridfunctions_f_infinity[NUM_EVOL_GFS] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.
 const char *bssn_b200_last_error(void) { return last_error(); }
 const char *bssn_b200_version(void) { return "bssn_b200 1.0 (sm_100a)"; }
 
+int bssn_b200_fd_order(void) { return BSSN_B200_FD_ORDER; }
+
 int bssn_b200_set_symmetry_axes(const char *axes) {
   int mask = 0;
   if (axes) {

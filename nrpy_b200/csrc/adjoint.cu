@@ -24,6 +24,9 @@
 
 #include "bssn_common.cuh"
 
+// The reverse-mode algebra and stencil transposes are generated for the 4th-order build only.
+#if BSSN_B200_FD_ORDER == 4
+
 namespace bssn {
 namespace {
 
@@ -929,3 +932,31 @@ int bssn_b200_adjoint_destroy(bssn_b200_adjoint *a) {
 }
 
 }  // extern "C"
+
+#else  // BSSN_B200_FD_ORDER != 4: the entry points exist and refuse
+
+namespace {
+int adjoint_unavailable() {
+  bssn::set_error("the adjoint is built for 4th-order finite differences only (this library: order %d)",
+                  BSSN_B200_FD_ORDER);
+  return BSSN_B200_EINVAL;
+}
+}  // namespace
+
+extern "C" {
+int bssn_b200_adjoint_create(commondata_struct *, griddata_struct *, int, int, void *, bssn_b200_adjoint **out) {
+  if (out) *out = nullptr;
+  return adjoint_unavailable();
+}
+int bssn_b200_adjoint_forward(bssn_b200_adjoint *, double *) { return adjoint_unavailable(); }
+int bssn_b200_adjoint_backward(bssn_b200_adjoint *, double, double *, double *) { return adjoint_unavailable(); }
+int bssn_b200_adjoint_functional(bssn_b200_adjoint *, const double *, double *) { return adjoint_unavailable(); }
+int bssn_b200_adjoint_functional_vjp(bssn_b200_adjoint *, const double *, double, double *) {
+  return adjoint_unavailable();
+}
+int bssn_b200_adjoint_step_vjp(bssn_b200_adjoint *, const double *, double *) { return adjoint_unavailable(); }
+int bssn_b200_adjoint_id_vjp(bssn_b200_adjoint *, const double *, double *) { return adjoint_unavailable(); }
+int bssn_b200_adjoint_destroy(bssn_b200_adjoint *) { return BSSN_B200_OK; }
+}  // extern "C"
+
+#endif  // BSSN_B200_FD_ORDER

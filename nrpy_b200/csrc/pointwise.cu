@@ -62,10 +62,19 @@ struct RegCtx {
 #define invdxx0 ctx.invdxx0
 #define invdxx1 ctx.invdxx1
 #define invdxx2 ctx.invdxx2
+#if BSSN_B200_FD_ORDER == 4
 #include "gen/bssn_sinh_3d.cuh"
 #include "gen/bssn_sinh_axi.cuh"
 #include "gen/bssn_sph_3d.cuh"
 #include "gen/bssn_sph_axi.cuh"
+#elif BSSN_B200_FD_ORDER == 8
+#include "gen/bssn_sinh_3d_fd8.cuh"
+#include "gen/bssn_sinh_axi_fd8.cuh"
+#include "gen/bssn_sph_3d_fd8.cuh"
+#include "gen/bssn_sph_axi_fd8.cuh"
+#else
+#error "BSSN_B200_FD_ORDER: generated algebra exists for 4 and 8"
+#endif
 #undef invdxx0
 #undef invdxx1
 #undef invdxx2

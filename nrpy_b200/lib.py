@@ -2,6 +2,11 @@
 
 The struct classes mirror the C layouts field by field. Loading fails loudly when the
 library has not been built: there is no fallback implementation.
+
+The interior finite-difference order is chosen per process by the environment variable
+BSSN_B200_FD_ORDER (4, the default: libbssn_b200.so; 8: libbssn_b200_fd8.so). NGHOSTS, and
+with it the bc_info_struct / bc_struct layouts, follow it; load() checks that the library was
+built for the same order.
 """
 
 import ctypes as C
@@ -9,7 +14,10 @@ import os
 import pathlib
 
 REAL = C.c_double
-NGHOSTS = 3
+FD_ORDER = int(os.environ.get("BSSN_B200_FD_ORDER", "4"))
+if FD_ORDER not in (4, 8):
+    raise ValueError(f"BSSN_B200_FD_ORDER={FD_ORDER}: libbssn_b200 is built for 4 and 8")
+NGHOSTS = FD_ORDER // 2 + 1
 NUM_EVOL_GFS = 24
 NUM_AUXEVOL_GFS = 6
 NUM_DIAG_GFS = 3
@@ -132,7 +140,8 @@ def _lib_path() -> pathlib.Path:
     env = os.environ.get("BSSN_B200_LIB")
     if env:
         return pathlib.Path(env)
-    return pathlib.Path(__file__).resolve().parent / "libbssn_b200.so"
+    name = "libbssn_b200.so" if FD_ORDER == 4 else f"libbssn_b200_fd{FD_ORDER}.so"
+    return pathlib.Path(__file__).resolve().parent / name
 
 
 _LIB = None
@@ -177,6 +186,7 @@ SIGNATURES = [
     ("bssn_b200_diagnostics", C.c_int, [PCD, PGD, V]),
     ("bssn_b200_last_error", C.c_char_p, []),
     ("bssn_b200_version", C.c_char_p, []),
+    ("bssn_b200_fd_order", C.c_int, []),
     ("bssn_b200_set_symmetry_axes", C.c_int, [C.c_char_p]),
     ("bssn_b200_ricci_eval", C.c_int, [PP, PRFM, PR, PR, V]),
     ("bssn_b200_rhs_eval", C.c_int, [PCD, PP, PRFM, PR, PR, PR, V]),
@@ -224,12 +234,15 @@ def load(path=None) -> C.CDLL:
         return _LIB
     p = pathlib.Path(path) if path else _lib_path()
     if not p.exists():
-        raise OSError(f"libbssn_b200.so not found at {p}; build it with `python -m nrpy_b200.build`")
+        raise OSError(f"{p.name} not found at {p}; build it with `python -m nrpy_b200.build --fd-order {FD_ORDER}`")
     lib = C.CDLL(str(p))
     for name, res, args in SIGNATURES:
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
+    if lib.bssn_b200_fd_order() != FD_ORDER:
+        raise OSError(f"{p} is built for fd_order {lib.bssn_b200_fd_order()}, this process expects {FD_ORDER} "
+                      "(BSSN_B200_FD_ORDER)")
     if path is None:
         _LIB = lib
     return lib

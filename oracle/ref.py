@@ -83,6 +83,7 @@ def _load(variant: str) -> C.CDLL:
     lib.ref_dV.argtypes = [vp, ip, ip, ip]
     lib.ref_diagnostics.argtypes = [vp, ip, C.c_double, C.c_double]
     lib.ref_initial_data.argtypes = [vp]
+    lib.ref_nghosts.argtypes = []
     lib.ref_set_clock.argtypes = [vp, ip, C.c_double]
     lib.ref_commondata.restype = vp
     lib.ref_commondata.argtypes = [vp]
@@ -124,6 +125,7 @@ class RefGrid:
                                      BH1_posn_z, BH2_mass, BH2_posn_z, CFL_FACTOR,
                                      1 if outer_bc_type == "extrapolation" else 0)
         self.N = tuple(self.lib.ref_N(self.h, d) for d in range(3))
+        self.nghosts = self.lib.ref_nghosts()
         self.ntot = self.N[0] * self.N[1] * self.N[2]
 
     def close(self):
@@ -235,7 +237,7 @@ class RefGrid:
         return self.lib.ref_checkpoint_every(self.h)
 
     def dV(self) -> np.ndarray:
-        G = NGHOSTS
+        G = self.nghosts
         out = np.zeros((self.N[2], self.N[1], self.N[0]))
         for i2 in range(G, self.N[2] - G):
             for i1 in range(G, self.N[1] - G):
@@ -254,7 +256,7 @@ class RefGrid:
         buf = (C.c_char * (ni * inner_dt.itemsize)).from_address(self.lib.ref_inner(self.h))
         inner = np.frombuffer(bytes(buf), dtype=inner_dt)
         outer = {}
-        for gz in range(NGHOSTS):
+        for gz in range(self.nghosts):
             for d in range(3):
                 n = self.lib.ref_num_pure_outer(self.h, gz, d)
                 if n:

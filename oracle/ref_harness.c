@@ -72,6 +72,7 @@ void ref_destroy(ref_sim *s) {
 
 // ---- sizes, layouts and raw pointers -------------------------------------------------
 size_t ref_sizeof_commondata(void) { return sizeof(commondata_struct); }
+int ref_nghosts(void) { return NGHOSTS; }
 size_t ref_sizeof_params(void) { return sizeof(params_struct); }
 size_t ref_sizeof_bc_struct(void) { return sizeof(bc_struct); }
 size_t ref_sizeof_griddata(void) { return sizeof(griddata_struct); }

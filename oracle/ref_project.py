@@ -12,7 +12,9 @@ nrpy/examples/two_blackholes_collide.py:60-440 with the settings the workloads n
 * every coordinate system's CodeParameters registered ("All"), so that one
   params_struct layout serves every project variant;
 * ``--checkpoint`` also registers write_checkpoint/read_checkpoint (checkpointing.py:473-490),
-  which adds the REAL CodeParameter checkpoint_every to commondata_struct.
+  which adds the REAL CodeParameter checkpoint_every to commondata_struct;
+* ``--fd-order N`` sets the interior finite-difference order (4 by default; NGHOSTS = N/2 + 1),
+  the outer radiation condition staying at radiation_BC_fd_order = 4.
 
 Run it with the reference on PYTHONPATH (oracle/gen_ref.py does this).
 """
@@ -33,6 +35,7 @@ ap.add_argument("--axisym", action="store_true")
 ap.add_argument("--project-dir", required=True)
 ap.add_argument("--cuda", action="store_true")
 ap.add_argument("--checkpoint", action="store_true")
+ap.add_argument("--fd-order", type=int, default=4)
 args = ap.parse_args()
 
 parallelization = "cuda" if args.cuda else "openmp"
@@ -51,7 +54,7 @@ if args.axisym:
 project_dir = args.project_dir
 shutil.rmtree(project_dir, ignore_errors=True)
 par.set_parval_from_str("enable_parallel_codegen", True)
-par.set_parval_from_str("fd_order", 4)
+par.set_parval_from_str("fd_order", args.fd_order)
 par.set_parval_from_str("CoordSystem_to_register_CodeParameters", "All")
 # Instantiate both reference metrics so that both register their CodeParameters
 # (RMAX for Spherical; AMPL, SINHW for SinhSpherical): every variant then shares one
