@@ -30,6 +30,11 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 NXX = (256, 64, 64)
+# Interior finite-difference order of this run (BSSN_B200_FD_ORDER: 4 by default, or 8 with
+# libbssn_b200_fd8.so); the reference arm and baselines use the reference project of the same order.
+FD_ORDER = int(os.environ.get("BSSN_B200_FD_ORDER", "4"))
+NG = FD_ORDER // 2 + 1
+SINH_VARIANT = "sinh3d" if FD_ORDER == 4 else f"sinh3d{FD_ORDER}"
 AMPL, SINHW = 10.0, 0.2
 H_EVERY = 20
 B_ALG_PER_PT_STEP = 3072  # bytes: classic RK4 with an accumulator, each stage read once
@@ -135,12 +140,12 @@ def cpu_reference_rate(steps_wanted: int, warmup: int, budget_s: float, seed: in
     """Reference generated OpenMP C (oracle/_ref), all host threads, on the same workload."""
     from oracle import ref
 
-    if not ref.available("sinh3d"):
+    if not ref.available(SINH_VARIANT):
         return None
     m1, z1, m2, z2 = bl_params(seed)
     cores = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    rg = ref.RefGrid("sinh3d", NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2)
+    rg = ref.RefGrid(SINH_VARIANT, NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2)
     for _ in range(max(1, min(warmup, 1))):
         rg.step(1)
     t0 = time.perf_counter()
@@ -155,6 +160,7 @@ def cpu_reference_rate(steps_wanted: int, warmup: int, budget_s: float, seed: in
     return {"value": pts * n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
             "kind": "reference",
             "sample": f"{n} RK4 steps of the full 256x64x64 SinhSpherical grid (reference generated OpenMP C, "
+                      f"fd_order {FD_ORDER}, "
                       f"MoL_step_forward_in_time incl. BCs + detgammabar), after 1 warm-up step",
             "s_per_step": dt / n}
 
@@ -166,7 +172,7 @@ def run_reference(args):
     budget = 150.0
     res = cpu_reference_rate(args.steps, args.warmup, budget, args.seed)
     if res is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/sinh3d not built (run oracle/gen_ref.py)"}))
+        print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/{SINH_VARIANT} not built (run oracle/gen_ref.py)"}))
         return
     line = {
         "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
@@ -283,8 +289,9 @@ def main():
     grid.close()
     del grid, y0, y_fp64
     torch.cuda.empty_cache()
-    batched = None if args.no_batched else run_batched(args, world, rank, dist)
-    differentiation = None if (args.no_diff or rank != 0) else run_differentiation()
+    # The batched path and the adjoint are tested at 4th order only (the adjoint is built only there).
+    batched = None if (args.no_batched or FD_ORDER != 4) else run_batched(args, world, rank, dist)
+    differentiation = None if (args.no_diff or rank != 0 or FD_ORDER != 4) else run_differentiation()
 
     if rank == 0:
         cpu = None
@@ -297,7 +304,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (Brill-Lindquist initial data, seeded)",
-            "config": {"workload": f"BSSN RK4, SinhSpherical {NXX[0]}x{NXX[1]}x{NXX[2]} (+3 ghosts), AMPL=10, SINHW=0.2, FP64, "
+            "config": {"workload": f"BSSN RK4, SinhSpherical {NXX[0]}x{NXX[1]}x{NXX[2]} (+{NG} ghosts), AMPL=10, SINHW=0.2, FP64, "
+                                   f"{FD_ORDER}th-order FD, "
                                    "KO, radiation BCs, H-constraint L2 every 20 steps",
                        "interior_points": pts, "mode": "fused stages" if args.mode == 1 else "reference stage order",
                        "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",
@@ -306,7 +314,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel, all output groups (one interior RK stage: RHS + RK4 update + projection)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
-                         "traffic": profiled_traffic() if NXX == (256, 64, 64) else None,
+                         "traffic": profiled_traffic() if NXX == (256, 64, 64) and FD_ORDER == 4 else None,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the two rhs group "
                                            "launches of one stage at 256x64x32, scaled by point count",
                          "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": kstats["ms_per_launch"],
@@ -459,9 +467,9 @@ def run_diagnostics(grid, args, reps: int = 3):
         try:
             from oracle import ref
 
-            if ref.available("sinh3d"):
+            if ref.available(SINH_VARIANT):
                 m1, z1, m2, z2 = bl_params(args.seed)
-                rg = ref.RefGrid("sinh3d", NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2,
+                rg = ref.RefGrid(SINH_VARIANT, NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2,
                                  BH2_posn_z=z2)
                 with tempfile.TemporaryDirectory() as d:
                     os.chdir(d)
