@@ -21,7 +21,8 @@ Variants
   sph3d  : Spherical, full 3-D (batched and adjoint workloads)
   sinh3d : SinhSpherical, full 3-D (the 256x64x64 workloads)
   sph3dck: sph3d plus write_checkpoint/read_checkpoint (checkpoint file parity)
-  sph3d8, sinh3d8: sph3d and sinh3d with 8th-order finite differences (NGHOSTS = 5)
+  sph3d8, sinh3d8, sphaxi8: sph3d, sinh3d and sphaxi with 8th-order finite differences
+           (NGHOSTS = 5)
 
 Usage: python oracle/gen_ref.py [--variants sphaxi,sph3d,sinh3d] [--reference DIR]
 """
@@ -43,6 +44,7 @@ VARIANTS = {
     "sph3dck": ["--coord", "Spherical", "--checkpoint"],
     "sph3d8": ["--coord", "Spherical", "--fd-order", "8"],
     "sinh3d8": ["--coord", "SinhSpherical", "--fd-order", "8"],
+    "sphaxi8": ["--coord", "Spherical", "--axisym", "--fd-order", "8"],
 }
 # Extra compiler definitions of a variant's harness build.
 HARNESS_DEFS = {"sph3dck": ["-DREF_HAS_CHECKPOINT"]}

@@ -43,14 +43,14 @@ def fd8_process():
     assert L.load().bssn_b200_fd_order() == 8
 
 
-def pair(variant, coord, Nxx, L, bh=(0.45, 0.5, 0.55, -0.6), outer="radiation"):
+def pair(variant, coord, Nxx, L, bh=(0.45, 0.5, 0.55, -0.6), outer="radiation", sym=""):
     from nrpy_b200.grid import BSSNGrid
 
     m1, z1, m2, z2 = bh
     rg = oref.RefGrid(variant, Nxx, L, SINHW=0.2, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2,
                       outer_bc_type=outer)
     g = BSSNGrid(coord=coord, Nxx=Nxx, grid_physical_size=L, SINHW=0.2, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2,
-                 BH2_posn_z=z2, outer_bc_type=outer)
+                 BH2_posn_z=z2, outer_bc_type=outer, symmetry_axes=sym)
     assert rg.nghosts == G and g.N == rg.N
     return rg, g
 
@@ -157,6 +157,52 @@ def test_sinh_steps_graph(cuda):
     g.free_stepper()
     rg.close()
     g.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_axisymmetric_100_steps(cuda, mode):
+    """Spherical 72x12x2, symmetry_axes='2' (the small workload at 8th order), 100 RK4 steps
+    from the reference's initial data."""
+    need("sphaxi8")
+    rg, g = pair("sphaxi8", "Spherical", (72, 12, 2), 7.5, bh=(0.5, 0.5, 0.5, -0.5), sym="2")
+    g.y_n.copy_(torch.from_numpy(rg.y_n()).to(g.device))
+    rg.step(100)
+    g.MoL_step_forward_in_time(mode=mode, nsteps=100)
+    torch.cuda.synchronize()
+    m = g.y_n.cpu().numpy().reshape(24, -1)
+    r = rg.y_n().reshape(24, -1)
+    num = np.sqrt(((m - r) ** 2).sum(axis=1))
+    den = np.sqrt((r**2).sum(axis=1))
+    err = num / np.maximum(den, 1e-13 * den.max())  # components that vanish analytically: against a floor
+    assert err.max() <= 1e-10, err
+    rg.close()
+    g.close()
+
+
+def test_batch_equals_single_grid_path(cuda):
+    """Two uneven Spherical grids advanced together by the batched persistent kernels, 4 RK4
+    steps, against each grid stepped alone."""
+    from nrpy_b200.batch import BatchedEvolutions
+    from nrpy_b200.grid import BSSNGrid
+
+    specs = [dict(coord="Spherical", Nxx=(24, 10, 6), grid_physical_size=7.5, BH1_mass=0.45, BH1_posn_z=0.35,
+                  BH2_mass=0.6, BH2_posn_z=-0.35),
+             dict(coord="Spherical", Nxx=(37, 12, 4), grid_physical_size=7.5, BH1_mass=0.31, BH1_posn_z=0.7,
+                  BH2_mass=0.66, BH2_posn_z=-0.7)]
+    be = BatchedEvolutions(specs)
+    be.build(tile=(32, 4), blocks=148, steps_per_graph=2)
+    be.run(2)
+    torch.cuda.synchronize()
+    for spec, g in zip(specs, be.grids):
+        single = BSSNGrid(**spec)
+        single.MoL_step_forward_in_time(mode=1, nsteps=4)
+        torch.cuda.synchronize()
+        a = single.y_n.view(24, -1).cpu().numpy()
+        b = g.y_n.view(24, -1).cpu().numpy()
+        err = rel_l2_per_gf(b, a, floor=1e-300)
+        assert np.nanmax(np.where(np.linalg.norm(a, axis=1) > 0, err, 0)) <= 1e-14, err
+        single.close()
+    be.close()
 
 
 def test_adjoint_refused(cuda):
