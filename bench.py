@@ -39,6 +39,9 @@ AMPL, SINHW = 10.0, 0.2
 H_EVERY = 20
 B_ALG_PER_PT_STEP = 3072  # bytes: classic RK4 with an accumulator, each stage read once
 STAGE_WORDS = (72, 120, 120, 72)  # per interior point, FP64 words, stages 1..4
+# FP64 operations per interior point of one fused stage pass (both RHS output groups, 2 DFMA +
+# DADD + DMUL), counted by ncu at 4th order: profiles/kernels_rhs_ricci_groups_sinh256x64x32.md.
+RHS_FLOP_PER_PT_STAGE = {4: 3458 + 2920}
 METRIC = "BSSN RK4 grid-point updates/s on 1 B200, FP64 vs mixed at equal H-error"
 UNIT = "pt-updates/s"
 
@@ -279,6 +282,15 @@ def main():
     peak, peak_kind = peaks()
     bytes_launch = np.mean(STAGE_WORDS) * 8 * pts
     achieved = bytes_launch / (kstats["ms_per_launch"] * 1e-3) / 1e9
+    fp64 = None
+    if FD_ORDER in RHS_FLOP_PER_PT_STAGE:
+        tf = C.c_double()
+        L.check(lib.bssn_b200_fp64_fma_rate(5, C.byref(tf), C.c_void_p(stream.cuda_stream)))
+        flop = RHS_FLOP_PER_PT_STAGE[FD_ORDER] * pts
+        fp64_achieved = flop / (kstats["ms_per_launch"] * 1e-3) / 1e12
+        fp64 = {"achieved": fp64_achieved, "peak": tf.value, "unit": "TFLOP/s", "frac": fp64_achieved / tf.value,
+                "flop_per_point": RHS_FLOP_PER_PT_STAGE[FD_ORDER],
+                "peak_source": "measured: independent FP64 FMA chains on every SM (bssn_b200_fp64_fma_rate)"}
 
     # ---------------- end-to-end through the public API with host buffers
     e2e = None if args.no_e2e else run_e2e(grid, args, y0)
@@ -320,7 +332,8 @@ def main():
                                            "launches of one stage at 256x64x32, scaled by point count",
                          "algorithmic_bytes_per_launch": bytes_launch, "ms_per_launch": kstats["ms_per_launch"],
                          "step_achieved": value / world * B_ALG_PER_PT_STEP / 1e9,
-                         "step_frac": value / world * B_ALG_PER_PT_STEP / 1e9 / peak},
+                         "step_frac": value / world * B_ALG_PER_PT_STEP / 1e9 / peak,
+                         "fp64": fp64},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "clocks": clocks,

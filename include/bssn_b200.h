@@ -473,6 +473,10 @@ int bssn_b200_read_checkpoint(commondata_struct *commondata, REAL *checkpoint_ev
 unsigned long long bssn_b200_kernel_launches(void);
 int bssn_b200_rhs_fused_stage(commondata_struct *commondata, griddata_struct *griddata, int stage, int mixed,
                               void *stream);
+/* FP64 FMA throughput of this GPU, as a roofline denominator for the FP64-bound point kernels:
+ * a kernel of independent FMA chains (no memory traffic) on every SM, timed with CUDA events,
+ * best of `reps` launches. out_tflops = 2 x FMAs / time, in TFLOP/s. Synchronises `stream`. */
+int bssn_b200_fp64_fma_rate(int reps, double *out_tflops, void *stream);
 
 /* Synchronous copy for callers without their own CUDA binding:
  * kind 0 = host->device, 1 = device->host, 2 = device->device. */

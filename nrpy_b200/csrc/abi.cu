@@ -64,6 +64,8 @@ int mol_step(commondata_struct *cd, griddata_struct *gd, int mode, int mixed, cu
 int fused_interior_stage(const commondata_struct *cd, griddata_struct *gd, int grid, int stage, int mixed,
                          cudaStream_t s);
 int mol_prepare(const commondata_struct *cd, griddata_struct *gd, int mode);
+// Instrumentation (reductions.cu)
+int fp64_fma_rate(int reps, double *out_tflops, cudaStream_t s);
 
 static int check_ptr(const void *p, const char *what) {
   if (!p) {
@@ -393,6 +395,15 @@ int bssn_b200_stepper_kernel_nodes(const bssn_b200_stepper *st, unsigned long lo
 }
 
 unsigned long long bssn_b200_kernel_launches(void) { return g_launches.load(); }
+
+int bssn_b200_fp64_fma_rate(int reps, double *out_tflops, void *stream) {
+  BSSN_TRY(check_ptr(out_tflops, "out_tflops"));
+  if (reps < 1 || reps > 100) {
+    set_error("reps=%d not in [1,100]", reps);
+    return BSSN_B200_EINVAL;
+  }
+  return fp64_fma_rate(reps, out_tflops, (cudaStream_t)stream);
+}
 
 int bssn_b200_rhs_fused_stage(commondata_struct *cd, griddata_struct *gd, int stage, int mixed, void *stream) {
   BSSN_TRY(check_ptr(cd, "commondata"));

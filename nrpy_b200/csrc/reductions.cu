@@ -204,4 +204,63 @@ int constraint_integrals_noalloc(const params_struct *p, const RfmArrays &rfm, c
   return BSSN_B200_OK;
 }
 
+
+// ---------------------------------------------------------------- FP64 FMA throughput
+// Eight independent FMA chains per thread keep every FP64 lane busy without memory traffic;
+// x <- x*a + b with |a| < 1 stays bounded. One double per block is stored so that the chains
+// are not removed.
+constexpr int FMA_THREADS = 256, FMA_CHAINS = 8, FMA_ITERS = 4096;
+
+__global__ void __launch_bounds__(FMA_THREADS) fma_chain_kernel(double *__restrict__ out, const double a,
+                                                                const double b) {
+  double x[FMA_CHAINS];
+#pragma unroll
+  for (int c = 0; c < FMA_CHAINS; c++) x[c] = 1e-3 * (threadIdx.x + c);
+  for (int i = 0; i < FMA_ITERS; i++) {
+#pragma unroll
+    for (int c = 0; c < FMA_CHAINS; c++) x[c] = fma(x[c], a, b);
+  }
+  double sum = 0.0;
+#pragma unroll
+  for (int c = 0; c < FMA_CHAINS; c++) sum += x[c];
+  if (threadIdx.x == 0) out[blockIdx.x] = sum;
+}
+
+int fp64_fma_rate(int reps, double *out_tflops, cudaStream_t s) {
+  int dev = 0, sms = 0;
+  BSSN_CUDA_TRY(cudaGetDevice(&dev));
+  BSSN_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int blocks = sms * 16;
+  double *out = nullptr;
+  BSSN_CUDA_TRY(cudaMalloc(&out, sizeof(double) * blocks));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = BSSN_B200_OK;
+  float best = 0.0f;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    set_error("fp64_fma_rate: event creation failed");
+    rc = BSSN_B200_ECUDA;
+  }
+  for (int r = -1; r < reps && rc == BSSN_B200_OK; r++) {  // r = -1: warm-up
+    cudaEventRecord(e0, s);
+    fma_chain_kernel<<<blocks, FMA_THREADS, 0, s>>>(out, 0.999999, 1e-7);
+    cudaEventRecord(e1, s);
+    if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+      set_error("fp64_fma_rate: kernel failed");
+      rc = BSSN_B200_ECUDA;
+      break;
+    }
+    count_launch(1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r >= 0 && (best == 0.0f || ms < best)) best = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(out);
+  if (rc != BSSN_B200_OK) return rc;
+  const double flop = 2.0 * FMA_CHAINS * (double)FMA_ITERS * FMA_THREADS * blocks;
+  *out_tflops = flop / (best * 1e-3) / 1e12;
+  return BSSN_B200_OK;
+}
+
 }  // namespace bssn
