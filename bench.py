@@ -506,39 +506,43 @@ def run_diagnostics(grid, args, reps: int = 3):
 
 def run_checkpoint(grid, args, reps: int = 3):
     """write_checkpoint / read_checkpoint of the bench grid's state (the reference's file format,
-    246 MB at 256x64x64): wall time per call, the restored state checked bit-for-bit; beside it
+    252 MB at 256x64x64): wall time per call, the restored state checked bit-for-bit; beside it
     the reference's own write_checkpoint / read_checkpoint (checkpoint-enabled project, same
-    grid size) on the host cores."""
+    grid size) on the host cores. Each side writes `reps` times, each time to a new file, then
+    reads `reps` times; best and median are reported, since the host's file system (page cache
+    or disk) sets much of the time."""
     import torch
 
     cwd = os.getcwd()
     res = {}
+
+    def timed(d, write, read):
+        wt, rt = [], []
+        for _ in range(reps):
+            for f in os.listdir(d):
+                os.remove(os.path.join(d, f))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            write()
+            wt.append(1e3 * (time.perf_counter() - t0))
+        size = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            read()
+            torch.cuda.synchronize()
+            rt.append(1e3 * (time.perf_counter() - t0))
+        return wt, rt, size
+
     y_saved = grid.y_n.clone()
     clock = (grid.cd.nn, grid.cd.time, grid.cd.t_0, grid.cd.nn_0)
     every = grid.cd.time if grid.cd.time > 0 else 1.0
     with tempfile.TemporaryDirectory() as d:
         os.chdir(d)
         try:
-            wt = []
-            for _ in range(reps):  # each write goes to a new file, as the reference's below
-                for f in os.listdir(d):
-                    os.remove(os.path.join(d, f))
-                torch.cuda.synchronize()
-                t0 = time.perf_counter()
-                grid.write_checkpoint(every)
-                wt.append(1e3 * (time.perf_counter() - t0))
-            res["write_ms"] = float(np.median(wt))
-            files = os.listdir(d)
-            res["file_bytes"] = os.path.getsize(os.path.join(d, files[0])) if files else 0
-            grid.y_n.zero_()
-            rt = []
-            for _ in range(reps):
-                t0 = time.perf_counter()
-                grid.read_checkpoint()
-                torch.cuda.synchronize()
-                rt.append(1e3 * (time.perf_counter() - t0))
-            res["read_ms"] = float(np.median(rt))
-            res["restored_bitwise"] = bool(torch.equal(grid.y_n, y_saved))
+            wt, rt, size = timed(d, lambda: grid.write_checkpoint(every), lambda: grid.read_checkpoint())
+            res.update({"write_ms": float(np.median(wt)), "write_ms_best": min(wt), "read_ms": float(np.median(rt)),
+                        "read_ms_best": min(rt), "file_bytes": size,
+                        "restored_bitwise": bool(torch.equal(grid.y_n, y_saved))})
         finally:
             os.chdir(cwd)
     grid.cd.nn, grid.cd.time, grid.cd.t_0, grid.cd.nn_0 = clock
@@ -550,16 +554,13 @@ def run_checkpoint(grid, args, reps: int = 3):
 
             if ref.available("sph3dck"):
                 rg = ref.RefGrid("sph3dck", NXX, 7.5)
+                rg.set_clock(1, rg.dt)
                 with tempfile.TemporaryDirectory() as d:
                     os.chdir(d)
                     try:
-                        rg.set_clock(1, rg.dt)
-                        t0 = time.perf_counter()
-                        rg.write_checkpoint(rg.dt)
-                        res["reference_write_ms"] = 1e3 * (time.perf_counter() - t0)
-                        t0 = time.perf_counter()
-                        rg.read_checkpoint()
-                        res["reference_read_ms"] = 1e3 * (time.perf_counter() - t0)
+                        wt, rt, _ = timed(d, lambda: rg.write_checkpoint(rg.dt), lambda: rg.read_checkpoint())
+                        res.update({"reference_write_ms": float(np.median(wt)), "reference_write_ms_best": min(wt),
+                                    "reference_read_ms": float(np.median(rt)), "reference_read_ms_best": min(rt)})
                     finally:
                         os.chdir(cwd)
                 rg.close()
