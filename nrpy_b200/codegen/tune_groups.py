@@ -54,6 +54,9 @@ LOW = [(60, True, True, 3), (48, True, True, 4)]
 LOW_GROUPS = {"ricci_0001", "ricci_0211", "ricci_1222", "rhs_a", "rhs_g1", "rhs_g2"}
 
 HARNESS_HEAD = r'''
+#ifndef TUNE_NG
+#define TUNE_NG 3
+#endif
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -86,11 +89,11 @@ struct PointCtx {
 #undef invdxx0
 #undef invdxx1
 #undef invdxx2
-constexpr int N0 = 262, N1 = 70, N2 = 38, NTOT = N0 * N1 * N2, MAXOUT = 18;
+constexpr int NG = TUNE_NG, N0 = 256 + 2 * NG, N1 = 64 + 2 * NG, N2 = 32 + 2 * NG, NTOT = N0 * N1 * N2, MAXOUT = 18;
 template <int NT, int MINB, int NOUT, class F>
 __global__ void __launch_bounds__(NT, MINB) kern(RfmArrays rfm, const double *in, const double *aux, double *out) {
-  const int i0 = 3 + blockIdx.x * 32 + threadIdx.x, i1 = 3 + blockIdx.y * (NT / 32) + threadIdx.y, i2 = 3 + blockIdx.z;
-  if (i0 >= N0 - 3 || i1 >= N1 - 3) return;
+  const int i0 = NG + blockIdx.x * 32 + threadIdx.x, i1 = NG + blockIdx.y * (NT / 32) + threadIdx.y, i2 = NG + blockIdx.z;
+  if (i0 >= N0 - NG || i1 >= N1 - NG) return;
   extern __shared__ double smem[];
   volatile double *sm = smem + threadIdx.x + 32 * threadIdx.y;
   const int idx = i0 + N0 * i1 + N0 * N1 * i2;
@@ -222,14 +225,16 @@ def generate_orders() -> None:
         print(tag, flush=True)
 
 
-def generate_caps(caps) -> None:
+def generate_caps(caps, fd_order: int = 4) -> None:
     """The present groups with their chosen allocation and order (generate.py) at several
-    register budgets."""
+    register budgets, at the given finite-difference order."""
     from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen import fdcoeffs as fdc
     from nrpy_b200.codegen.emit_cuda import emit_point_function
     from nrpy_b200.codegen.generate import RHS_ALLOC, RICCI_ALLOC
 
-    be.setup_nrpy("")
+    fdc.set_fd_order(fd_order)
+    be.setup_nrpy("", fd_order)
     rhs, betaU = be.rhs_exprs("SinhSpherical")
     ricci = be.ricci_exprs("SinhSpherical")
     OUT.mkdir(parents=True, exist_ok=True)
@@ -249,9 +254,10 @@ def generate_caps(caps) -> None:
                             f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
             nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
             calls.append(f'  run<{nt}, 1, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
-        tag = f"caps_{gname}"
+        tag = f"caps_{gname}" if fd_order == 4 else f"caps{fd_order}_{gname}"
         (OUT / f"{tag}.cuh").write_text("\n".join(parts))
-        head, main = HARNESS_HEAD.replace("GROUP", tag).split("int main() {")
+        head, main = HARNESS_HEAD.replace("GROUP", tag).replace("#define TUNE_NG 3", f"#define TUNE_NG {fdc.NGHOSTS}"
+                                                                 ).split("int main() {")
         (OUT / f"{tag}.cu").write_text(head + "\n".join(wrappers) + "\nint main() {" + main + "\n".join(calls)
                                         + "\n  return 0;\n}\n")
         print(tag, flush=True)
@@ -282,9 +288,10 @@ def generate_leaf() -> None:
          "double *leafout;"),
         ("#define LDAUX(k) ctx.ldaux(k)", "#define LDAUX(k) ctx.ldaux(k)\n#define LDLEAF(k) __ldg(ctx.leaf + (size_t)(k) * NTOT)"
          "\n#define LEAFOUT(k, v) ctx.leafout[(size_t)(k) * NTOT] = (v)"),
-        ("constexpr int N0 = 262, N1 = 70, N2 = 38, NTOT = N0 * N1 * N2, MAXOUT = 18;\n", ""),
-        ('#include "GROUP.cuh"', 'constexpr int N0 = 262, N1 = 70, N2 = 38, NTOT = N0 * N1 * N2, MAXOUT = 18;\n'
-         '#include "GROUP.cuh"'),
+        ("constexpr int NG = TUNE_NG, N0 = 256 + 2 * NG, N1 = 64 + 2 * NG, N2 = 32 + 2 * NG, NTOT = N0 * N1 * N2, "
+         "MAXOUT = 18;\n", ""),
+        ('#include "GROUP.cuh"', 'constexpr int NG = TUNE_NG, N0 = 256 + 2 * NG, N1 = 64 + 2 * NG, N2 = 32 + 2 * NG, '
+         'NTOT = N0 * N1 * N2, MAXOUT = 18;\n#include "GROUP.cuh"'),
         ("ctx.KreissOliger_strength_nongauge = 0.3;",
          "ctx.KreissOliger_strength_nongauge = 0.3; ctx.leaf = g_leaf + idx; ctx.leafout = g_leaf + idx;"),
         ("template <int NT, int MINB, int NOUT, class F>\n__global__",
@@ -365,6 +372,7 @@ if __name__ == "__main__":
     ap.add_argument("step", choices=["generate", "generate-orders", "generate-caps", "generate-leaf", "compile", "run",
                                      "summarize"])
     ap.add_argument("--caps", default="72,80,90,100")
+    ap.add_argument("--fd-order", type=int, default=4)
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--log", default=None)
     a = ap.parse_args()
@@ -373,7 +381,7 @@ if __name__ == "__main__":
     elif a.step == "generate-orders":
         generate_orders()
     elif a.step == "generate-caps":
-        generate_caps([int(c) for c in a.caps.split(",")])
+        generate_caps([int(c) for c in a.caps.split(",")], a.fd_order)
     elif a.step == "generate-leaf":
         generate_leaf()
     elif a.step == "compile":
