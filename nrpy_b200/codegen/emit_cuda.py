@@ -550,14 +550,13 @@ def emit_point_function(
     deriv_remat: bool = False,
     order: str = "dfs",
     leaf_index: Optional[Dict[str, int]] = None,
-    volatile_slots: bool = True,
 ) -> Tuple[str, Dict[str, int]]:
     """Emit `fname` and the constant `fname_SMEM_SLOTS`. With reg_capacity > 0 the values
     beyond that many live doubles go to shared-memory slots (SMEM(k), provided by the
     caller through the `sm` argument: slot k of this thread; the template parameter NT is
-    the slot stride, i.e. the threads of a block). With volatile_slots the slot array is
-    volatile, so every slot access is a shared-memory access at its place in the program;
-    otherwise the compiler may move and merge them (each thread only touches its own slots)."""
+    the slot stride, i.e. the threads of a block). The slot pointer type S is the caller's:
+    `volatile T` keeps every slot access a shared-memory access at its place in the program,
+    plain `T` lets the compiler move and merge them (each thread only touches its own slots)."""
     pk = PointKernel(symmetry_axes, leaf_index)
     pk.build(outputs, upwind_vec)
     if reg_capacity > 0:
@@ -572,9 +571,8 @@ def emit_point_function(
     head = f"// {comment}\n" if comment else ""
     code = (
         f"{head}constexpr int {fname}_SMEM_SLOTS = {nslots};\n"
-        f"template <typename T, typename TF, int NT = 128, typename Ctx>\n"
-        f"__device__ __forceinline__ void {fname}(const Ctx &ctx, T *__restrict__ out, "
-        f"{'volatile T' if volatile_slots else 'T'} *sm) {{\n"
+        f"template <typename T, typename TF, int NT = 128, typename Ctx, typename S>\n"
+        f"__device__ __forceinline__ void {fname}(const Ctx &ctx, T *__restrict__ out, S *sm) {{\n"
         f"  (void)sm;\n{body}\n}}\n"
     )
     stats = dict(pk.stats)

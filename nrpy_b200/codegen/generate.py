@@ -59,10 +59,11 @@ RHS_ALLOC = [(True, False, "dfs"), (True, False, "sched")]
 # stencil loads) even with a few local-memory spills.
 RICCI_CAPS = [160, 150]
 RHS_CAPS = [72, 80]
-# Whether a group's slot array is volatile (every slot access stays where the allocator put
-# it) or plain (the compiler may schedule the accesses): per group, from a timing sweep.
-RICCI_VOLATILE = [True, True]
-RHS_VOLATILE = [True, True]
+# Value types for which a group's slot array is plain instead of volatile (volatile: every slot
+# access stays where the allocator put it; plain: the compiler may schedule the accesses), per
+# group, from a timing sweep: plain slots help the RHS groups in FP32 and cost in FP64.
+RICCI_PLAIN_SLOTS = [(), ()]
+RHS_PLAIN_SLOTS = [("float",), ("float",)]
 # Threads per block of a group kernel: 128, or 64 when two 128-thread blocks of its
 # shared-memory slots would not fit in the 227 KB of one SM.
 SMEM_PER_SM = 227 * 1024
@@ -85,11 +86,12 @@ ADJ_REG_CAPACITY = 150
 ADJ_REMAT = dict(remat_first=True, deriv_remat=True, order="sched_dfs")
 
 
-def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int, volatile_slots: bool = True) -> str:
+def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int, plain_slots=()) -> str:
     cases = " ".join(f"case {k}: return {x};" for k, x in enumerate(gfs))
-    # The kernels hand every group a volatile slot pointer; a group with plain slots gets it
-    # without the qualifier (the dynamic shared memory itself is not a volatile object).
-    arg = "sm" if volatile_slots else "const_cast<T *>(sm)"
+    # The kernels hand every group a volatile slot pointer; for the value types listed in
+    # plain_slots the group passes it on without the qualifier (the dynamic shared memory
+    # itself is not a volatile object).
+    plain = " || ".join(f"std::is_same<T, {t}>::value" for t in plain_slots) or "false"
     return (
         f"template <> struct {kind}_{tag}<{g}> {{\n"
         f"  static constexpr int N = {len(gfs)};\n"
@@ -99,7 +101,11 @@ def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int, vola
         f"    switch (k) {{ {cases} }}\n    return -1;\n  }}\n"
         f"  template <typename T, typename TF, int NTB, typename Ctx>\n"
         f"  __device__ __forceinline__ static void eval(const Ctx &ctx, T *out, volatile T *sm) {{\n"
-        f"    {fname}<T, TF, NTB>(ctx, out, {arg});\n  }}\n}};\n"
+        f"    if constexpr ({plain}) {{\n"
+        f"      {fname}<T, TF, NTB>(ctx, out, const_cast<T *>(sm));\n"
+        f"    }} else {{\n"
+        f"      {fname}<T, TF, NTB>(ctx, out, sm);\n"
+        f"    }}\n  }}\n}};\n"
     )
 
 
@@ -132,12 +138,11 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
             fname, [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
             comment=f"Rbar_ij {names}, {coord} (symmetry_axes='{sym}'): Ricci_eval.py:27-167",
             reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
-            volatile_slots=RICCI_VOLATILE[g],
         )
         parts.append(code)
         stats[f"ricci_g{g}"] = st
         structs.append(_group_struct("RicciGroup", tag, g, fname, [be.RBAR_ORDER.index(k) for k in names],
-                                     st["smem_slots"], RICCI_VOLATILE[g]))
+                                     st["smem_slots"], RICCI_PLAIN_SLOTS[g]))
     for g, names in enumerate(RHS_GROUPS):
         fname = f"rhs_point_{tag}_g{g}"
         remat_first, deriv_remat, order = RHS_ALLOC[g]
@@ -146,12 +151,11 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
             fname, [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU, symmetry_axes=sym,
             comment=f"BSSN RHS + KO (CAKO) of {names}, {coord} (symmetry_axes='{sym}'): rhs_eval.py:122-220",
             reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
-            volatile_slots=RHS_VOLATILE[g],
         )
         parts.append(code)
         stats[f"rhs_g{g}"] = st
         structs.append(_group_struct("RhsGroup", tag, g, fname, [be.GF_ORDER.index(k) for k in names],
-                                     st["smem_slots"], RHS_VOLATILE[g]))
+                                     st["smem_slots"], RHS_PLAIN_SLOTS[g]))
     code, st = emit_point_function(
         f"constraints_point_{tag}",
         [(f"out[{i}]", cons[k]) for i, k in enumerate(["H", "MSQUARED", "LAMBDA_CONSTRAINT"])],
@@ -185,7 +189,7 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', {fd_order}th-order FD, KO (CAKO).\n"
         f"// Register budgets Ricci {RICCI_CAPS}, RHS {RHS_CAPS} values; allocation (remat_first, deriv_remat, "
-        f"order): Ricci {RICCI_ALLOC}, RHS {RHS_ALLOC}; volatile slots Ricci {RICCI_VOLATILE}, RHS {RHS_VOLATILE}.\n"
+        f"order): Ricci {RICCI_ALLOC}, RHS {RHS_ALLOC}; plain slots Ricci {RICCI_PLAIN_SLOTS}, RHS {RHS_PLAIN_SLOTS}.\n"
         f"// Per point: {stats}\n"
         "#pragma once\n\n"
     )

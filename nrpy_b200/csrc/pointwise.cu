@@ -109,12 +109,14 @@ static int for_each_group(F &&f) {
   }
 }
 
+// Point functions without shared-memory slots get a typed null slot pointer.
+#define NOSLOTS(T) static_cast<volatile T *>(nullptr)
 #define DISPATCH_POINT(NAME, V, T, TF, CTX, OUT)                                  \
   do {                                                                            \
-    if constexpr (V == SPH_3D) NAME##_sph_3d<T, TF>(CTX, OUT, nullptr);           \
-    else if constexpr (V == SPH_AXI) NAME##_sph_axi<T, TF>(CTX, OUT, nullptr);    \
-    else if constexpr (V == SINH_3D) NAME##_sinh_3d<T, TF>(CTX, OUT, nullptr);    \
-    else NAME##_sinh_axi<T, TF>(CTX, OUT, nullptr);                               \
+    if constexpr (V == SPH_3D) NAME##_sph_3d<T, TF>(CTX, OUT, NOSLOTS(T));        \
+    else if constexpr (V == SPH_AXI) NAME##_sph_axi<T, TF>(CTX, OUT, NOSLOTS(T)); \
+    else if constexpr (V == SINH_3D) NAME##_sinh_3d<T, TF>(CTX, OUT, NOSLOTS(T)); \
+    else NAME##_sinh_axi<T, TF>(CTX, OUT, NOSLOTS(T));                            \
   } while (0)
 
 __device__ __forceinline__ PointCtx make_ctx(const GridDims &g, const RfmArrays &rfm, const double *in,
