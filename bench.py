@@ -168,6 +168,12 @@ def cpu_reference_rate(steps_wanted: int, warmup: int, budget_s: float, seed: in
             "s_per_step": dt / n}
 
 
+def workload_name() -> str:
+    """The workload both arms run (the same string in both JSON lines)."""
+    return (f"BSSN RK4, SinhSpherical {NXX[0]}x{NXX[1]}x{NXX[2]} (+{NG} ghosts), AMPL=10, SINHW=0.2, FP64, "
+            f"{FD_ORDER}th-order FD, KO, radiation BCs, H-constraint L2 every 20 steps")
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -182,7 +188,9 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["s_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (Brill-Lindquist initial data, seeded)",
-        "config": {"workload": "BSSN RK4, SinhSpherical 256x64x64 (+3 ghosts), AMPL=10, SINHW=0.2, KO, radiation BCs"},
+        "config": {"workload": workload_name(), "interior_points": NXX[0] * NXX[1] * NXX[2],
+                   "parallelism": "reference generated OpenMP C on the host cores (rank 0 only)", "seed": args.seed,
+                   "bl": list(bl_params(args.seed))},
         "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -317,9 +325,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (Brill-Lindquist initial data, seeded)",
-            "config": {"workload": f"BSSN RK4, SinhSpherical {NXX[0]}x{NXX[1]}x{NXX[2]} (+{NG} ghosts), AMPL=10, SINHW=0.2, FP64, "
-                                   f"{FD_ORDER}th-order FD, "
-                                   "KO, radiation BCs, H-constraint L2 every 20 steps",
+            "config": {"workload": workload_name(),
                        "interior_points": pts, "mode": "fused stages" if args.mode == 1 else "reference stage order",
                        "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",
                        "parallelism": f"replicas x{world}", "seed": args.seed, "bl": [m1, z1, m2, z2],
