@@ -459,7 +459,8 @@ int bssn_b200_write_checkpoint(const commondata_struct *commondata, REAL checkpo
 /* read_checkpoint (checkpointing.py:15-243). Returns 0 when the file does not exist, 1 when it was
  * read, a negative code on failure (the reference exits instead). commondata is overwritten with the
  * file's values, then t_0 = time and nn_0 = nn; checkpoint_every (may be NULL) receives the file's
- * cadence. griddata == NULL reads only commondata (to rebuild the grids first). Otherwise each grid's
+ * cadence. griddata == NULL reads only commondata (to rebuild the grids first). Otherwise griddata
+ * must hold the file's NUMGRIDS grids, as for the reference's read_checkpoint, and each grid's
  * saved params must match its Nxx_plus_2NGHOSTS* and CoordSystem_hash, count must lie in [0, ntot] and
  * every index in [0, ntot); y_n_gfs (device, already allocated) is zeroed and the saved points are
  * scattered into it on the GPU. */
