@@ -10,7 +10,8 @@ timed region). Synthetic data: the Brill-Lindquist initial data computed in-proc
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 (under torchrun): independent replicas, one per GPU (a single evolution does not
-shard without a halo exchange), each with its own seed; value is the
+shard without a halo exchange of 3 ghost layers x 24 gridfunctions per stage, and the inner
+parity map crosses the axis), each with its own seed; value is the
 whole-job rate = sum of all ranks' point updates / max over ranks of the device time.
 """
 

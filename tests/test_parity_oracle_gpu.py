@@ -1,7 +1,7 @@
 """GPU parity against the live reference oracle (oracle/_ref: the reference's own generated
 BHaH C, compiled by oracle/gen_ref.py) at the workload sizes.
 
-Bars (from the north star): per-gridfunction relative L2 <= 1e-12 after one FP64 RHS,
+Bars: per-gridfunction relative L2 <= 1e-12 after one FP64 RHS,
 <= 1e-10 after 100 FP64 RK4 steps. Starting states are the reference's own initial data
 (so that rounding differences of the two initial-data codes do not enter), or the
 reference's data plus seeded smooth perturbations of all 24 gridfunctions.
