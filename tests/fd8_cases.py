@@ -205,6 +205,66 @@ def test_batch_equals_single_grid_path(cuda):
     be.close()
 
 
+def _read(path):
+    comments, rows = [], []
+    for line in path.read_text().splitlines():
+        (comments if line.startswith("#") else rows).append(line)
+    return comments, np.array([[float(x) for x in r.split()] for r in rows])
+
+
+def test_diagnostics_files_match_reference(cuda, tmp_path, monkeypatch):
+    """The diagnostics() outputs (nearest-point samples, volume integrals) of a perturbed
+    8th-order state against the reference's own diagnostics() at fd_order 8."""
+    need("sph3d8")
+    rg, g = pair("sph3d8", "Spherical", (24, 12, 12), 7.5)
+    state = oref.perturbed_state(rg, seed=4)
+    rg.set_y_n(state)
+    g.y_n.copy_(torch.from_numpy(state).to(g.device))
+    for d in ("ref", "ours"):
+        (tmp_path / d).mkdir()
+    monkeypatch.chdir(tmp_path / "ref")
+    rg.diagnostics(0, 0.0, 0.25)
+    monkeypatch.chdir(tmp_path / "ours")
+    g.diagnostics(0.25, nn=0, time=0.0)
+    torch.cuda.synchronize()
+    monkeypatch.chdir(tmp_path)
+    names = sorted(p.name for p in (tmp_path / "ref").iterdir())
+    assert names and sorted(p.name for p in (tmp_path / "ours").iterdir()) == names
+    for name in names:
+        c_ref, d_ref = _read(tmp_path / "ref" / name)
+        c_ours, d_ours = _read(tmp_path / "ours" / name)
+        assert c_ours == c_ref and d_ours.shape == d_ref.shape, name
+        if name.startswith("out3d"):
+            np.testing.assert_allclose(d_ours, d_ref, rtol=1e-10, atol=0, err_msg=name)
+            continue
+        nc = 1 if name.startswith(("out0d", "out1d")) else 2
+        np.testing.assert_allclose(d_ours[:, :nc], d_ref[:, :nc], rtol=1e-12, atol=1e-12, err_msg=name)
+        scale = np.abs(d_ref[:, nc:]).max(axis=0)
+        assert np.all(np.abs(d_ours[:, nc:] - d_ref[:, nc:]) <= 1e-9 * scale + 1e-300), name
+    rg.close()
+    g.close()
+
+
+def test_checkpoint_restart_bitwise(cuda, tmp_path, monkeypatch):
+    """A run restarted from a checkpoint (5 ghost layers) continues bit-identically."""
+    monkeypatch.chdir(tmp_path)
+    from nrpy_b200.grid import BSSNGrid
+
+    kw = dict(coord="Spherical", Nxx=(24, 12, 12), grid_physical_size=7.5)
+    a = BSSNGrid(**kw)
+    a.MoL_step_forward_in_time(nsteps=4)
+    b = BSSNGrid(**kw)
+    b.MoL_step_forward_in_time(nsteps=2)
+    assert b.write_checkpoint(b.cd.time)
+    c = BSSNGrid(**kw, initial_data=False)
+    assert c.read_checkpoint() is not None
+    c.MoL_step_forward_in_time(nsteps=2)
+    torch.cuda.synchronize()
+    assert torch.equal(a.y_n, c.y_n) and c.cd.nn == 4
+    for x in (a, b, c):
+        x.close()
+
+
 def test_adjoint_refused(cuda):
     import ctypes as C
 
