@@ -92,3 +92,24 @@ def test_reference_checkpoint_cadence(tmp_path, monkeypatch):
     rg.write_checkpoint(0.0)  # checkpoint_every <= 0: never
     assert not list(tmp_path.glob("checkpoint-*.dat"))
     rg.close()
+
+
+def test_library_reads_reference_commondata_without_gpu(tmp_path, monkeypatch):
+    """bssn_b200_read_checkpoint with griddata = NULL touches no GPU: it reads the commondata
+    of a file written by the reference's write_checkpoint; without a file it returns 0."""
+    ref = _ref("sph3dck")
+    lib = L.load()
+    monkeypatch.chdir(tmp_path)
+    cd = L.CommondataStruct()
+    cd.convergence_factor = 1.0
+    every = L.REAL()
+    assert lib.bssn_b200_read_checkpoint(C.byref(cd), C.byref(every), None, None) == 0  # no file yet
+    assert lib.bssn_b200_read_checkpoint(None, None, None, None) == -1  # BSSN_B200_EINVAL
+    rg = ref.RefGrid("sph3dck", (8, 4, 4), 7.5, BH1_mass=0.45, BH2_posn_z=-0.35)
+    rg.step(3)
+    t, nn, dt = rg.time, rg.nn(), rg.dt
+    rg.write_checkpoint(t)
+    rg.close()
+    assert lib.bssn_b200_read_checkpoint(C.byref(cd), C.byref(every), None, None) == 1
+    assert (cd.time, cd.nn, cd.dt, every.value) == (t, nn, dt, t)
+    assert (cd.BH1_mass, cd.BH2_posn_z, cd.NUMGRIDS, cd.outer_bc_type) == (0.45, -0.35, 1, b"radiation")
