@@ -88,10 +88,10 @@ ADJ_REMAT = dict(remat_first=True, deriv_remat=True, order="sched_dfs")
 
 def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int, plain_slots=()) -> str:
     cases = " ".join(f"case {k}: return {x};" for k, x in enumerate(gfs))
-    # The kernels hand every group a volatile slot pointer; for the value types listed in
-    # plain_slots the group passes it on without the qualifier (the dynamic shared memory
-    # itself is not a volatile object).
-    plain = " || ".join(f"std::is_same<T, {t}>::value" for t in plain_slots) or "false"
+    # The kernels hand a group a volatile slot pointer, or a plain one to ask for plain slots;
+    # for the value types listed in plain_slots the group drops the qualifier itself (the
+    # dynamic shared memory is not a volatile object).
+    plain = " || ".join(["!std::is_volatile<S>::value"] + [f"std::is_same<T, {t}>::value" for t in plain_slots])
     return (
         f"template <> struct {kind}_{tag}<{g}> {{\n"
         f"  static constexpr int N = {len(gfs)};\n"
@@ -99,8 +99,8 @@ def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int, plai
         f"  static constexpr int NT = {threads_for(slots)};  // threads per block of the single-grid kernels\n"
         f"  __host__ __device__ static constexpr int GF(int k) {{\n"
         f"    switch (k) {{ {cases} }}\n    return -1;\n  }}\n"
-        f"  template <typename T, typename TF, int NTB, typename Ctx>\n"
-        f"  __device__ __forceinline__ static void eval(const Ctx &ctx, T *out, volatile T *sm) {{\n"
+        f"  template <typename T, typename TF, int NTB, typename Ctx, typename S>\n"
+        f"  __device__ __forceinline__ static void eval(const Ctx &ctx, T *out, S *sm) {{\n"
         f"    if constexpr ({plain}) {{\n"
         f"      {fname}<T, TF, NTB>(ctx, out, const_cast<T *>(sm));\n"
         f"    }} else {{\n"

@@ -180,9 +180,10 @@ __device__ __forceinline__ volatile T *thread_slots() {
   return reinterpret_cast<volatile T *>(smem_raw) + (threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z));
 }
 
-template <Variant V, int G, typename T, int NTB>
+// S: the slot element type, volatile T or plain T (see the group's eval).
+template <Variant V, int G, typename T, int NTB, typename S>
 __device__ __forceinline__ void ricci_body(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux,
-                                           int i0, int i1, int i2, volatile T *sm) {
+                                           int i0, int i1, int i2, S *sm) {
   using Grp = RicciG<V, G>;
   const PointCtx ctx = make_ctx(g, rfm, in, nullptr, i0, i1, i2);
   T out[Grp::N];
@@ -306,10 +307,10 @@ __device__ __forceinline__ void rk_and_project_point(const GridDims &g, const Rf
 // of that group's gridfunctions; the group holding hDD also applies the detgammabar
 // projection to the new hDD. The raw RHS is also stored to `krhs` on the interior shell
 // (the layer next to each face), where the outer radiation condition reads it.
-template <Variant V, typename T, int STAGE, int G, int NTB>
+template <Variant V, typename T, int STAGE, int G, int NTB, typename S>
 __device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
                                            const double *aux, const StageBuffers &b, double *krhs, const double dt,
-                                           int i0, int i1, int i2, volatile T *sm) {
+                                           int i0, int i1, int i2, S *sm) {
   using Grp = RhsG<V, G>;
   PointCtx ctx = make_ctx(g, rfm, b.kin, aux, i0, i1, i2);
   ctx.eta = pp.eta;
@@ -589,7 +590,8 @@ __global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_fused_batched_kernel(co
                                                                             const int ntiles, const int bx,
                                                                             const int by) {
   constexpr int NT = RhsG<V, G>::NT;
-  volatile double *sm = thread_slots<double>();
+  // Plain slots: in the persistent batched kernels the RHS groups ran faster with them.
+  double *sm = const_cast<double *>(thread_slots<double>());
   for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const EvoDesc &d = descs[tile_evo[t]];
     StageBuffers b;
