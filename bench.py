@@ -140,33 +140,80 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference_rate(steps_wanted: int, warmup: int, budget_s: float, seed: int):
-    """Reference generated OpenMP C (oracle/_ref), all host threads, on the same workload."""
+def host_cpu():
+    """The host CPU as lscpu reports it: model, physical cores (cores per socket x sockets,
+    capped by this process's CPU affinity) and logical CPUs."""
+    info = {"model": None, "physical_cores": None, "logical_cpus": os.cpu_count()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        kv = {}
+        for line in out.splitlines():
+            if ":" in line:
+                k, v = line.split(":", 1)
+                kv[k.strip()] = v.strip()
+        info["model"] = kv.get("Model name")
+        cps, sock = int(kv.get("Core(s) per socket", "0")), int(kv.get("Socket(s)", "1") or 1)
+        info["threads_per_core"] = int(kv.get("Thread(s) per core", "1") or 1)
+        if cps > 0:
+            info["physical_cores"] = cps * sock
+    except (OSError, ValueError, subprocess.SubprocessError):
+        pass
+    if not info["physical_cores"]:
+        try:
+            import psutil
+
+            info["physical_cores"] = psutil.cpu_count(logical=False)
+        except Exception:  # noqa: BLE001
+            info["physical_cores"] = os.cpu_count()
+    try:
+        aff = len(os.sched_getaffinity(0))
+        info["affinity_cpus"] = aff
+        tpc = info.get("threads_per_core", 1) or 1
+        info["physical_cores"] = max(1, min(info["physical_cores"], aff // tpc if aff >= tpc else aff))
+    except (AttributeError, OSError):
+        pass
+    return info
+
+
+def set_reference_threads():
+    """OpenMP settings of the reference's CPU runs: one thread per physical core, bound close
+    (set before the reference library is loaded, which reads them at start-up)."""
+    cpu = host_cpu()
+    os.environ["OMP_NUM_THREADS"] = str(cpu["physical_cores"])
+    os.environ["OMP_PROC_BIND"] = "close"
+    os.environ["OMP_PLACES"] = "cores"
+    return cpu
+
+
+def cpu_reference_rate(steps: int, warmup: int, runs: int, seed: int):
+    """The reference's generated OpenMP C (oracle/_ref) on the same workload, on all physical
+    host cores: `warmup` untimed RK4 steps, then `runs` timed runs of `steps` steps each
+    (MoL_step_forward_in_time only); the median run is reported."""
+    cpu = set_reference_threads()
     from oracle import ref
 
     if not ref.available(SINH_VARIANT):
         return None
     m1, z1, m2, z2 = bl_params(seed)
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
     rg = ref.RefGrid(SINH_VARIANT, NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2)
-    for _ in range(max(1, min(warmup, 1))):
-        rg.step(1)
-    t0 = time.perf_counter()
-    rg.step(1)
-    t1 = time.perf_counter() - t0
-    n = max(1, min(steps_wanted, int(budget_s / max(t1, 1e-9))))
-    t0 = time.perf_counter()
-    rg.step(n)
-    dt = time.perf_counter() - t0
+    if warmup > 0:
+        rg.step(warmup)
+    times = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        rg.step(steps)
+        times.append(time.perf_counter() - t0)
     rg.close()
+    dt = float(np.median(times))
     pts = NXX[0] * NXX[1] * NXX[2]
-    return {"value": pts * n / dt, "unit": UNIT, "cores": int(os.environ.get("OMP_NUM_THREADS", cores)),
+    return {"value": pts * steps / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
             "kind": "reference",
-            "sample": f"{n} RK4 steps of the full 256x64x64 SinhSpherical grid (reference generated OpenMP C, "
-                      f"fd_order {FD_ORDER}, "
-                      f"MoL_step_forward_in_time incl. BCs + detgammabar), after 1 warm-up step",
-            "s_per_step": dt / n}
+            "sample": f"median of {runs} runs of {steps} RK4 steps of the full {NXX[0]}x{NXX[1]}x{NXX[2]} "
+                      f"SinhSpherical grid after {warmup} warm-up steps (reference generated OpenMP C, fd_order "
+                      f"{FD_ORDER}, MoL_step_forward_in_time incl. BCs + detgammabar; OMP_NUM_THREADS = physical "
+                      f"cores, OMP_PROC_BIND=close)",
+            "s_per_step": dt / steps, "run_s": times, "cpu_model": cpu.get("model"),
+            "physical_cores": cpu.get("physical_cores"), "logical_cpus": cpu.get("logical_cpus")}
 
 
 def workload_name() -> str:
@@ -175,12 +222,17 @@ def workload_name() -> str:
             f"{FD_ORDER}th-order FD, KO, radiation BCs, H-constraint L2 every 20 steps")
 
 
+def bench_config(seed: int, world: int):
+    """The workload description both arms print (identical keys and values)."""
+    return {"workload": workload_name(), "interior_points": NXX[0] * NXX[1] * NXX[2], "H_every": H_EVERY,
+            "parallelism": f"replicas x{world}", "seed": seed, "bl": list(bl_params(seed))}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    budget = 150.0
-    res = cpu_reference_rate(args.steps, args.warmup, budget, args.seed)
+    res = cpu_reference_rate(args.steps, 5, 3, args.seed)
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": f"oracle/_ref/{SINH_VARIANT} not built (run oracle/gen_ref.py)"}))
         return
@@ -189,10 +241,10 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * res["s_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (Brill-Lindquist initial data, seeded)",
-        "config": {"workload": workload_name(), "interior_points": NXX[0] * NXX[1] * NXX[2],
-                   "parallelism": "reference generated OpenMP C on the host cores (rank 0 only)", "seed": args.seed,
-                   "bl": list(bl_params(args.seed))},
-        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "config": bench_config(args.seed, args.gpus),
+        "implementation": "reference generated OpenMP C on the host cores (rank 0 only)",
+        "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model",
+                                             "physical_cores", "logical_cpus", "run_s")},
         "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -221,6 +273,9 @@ def main():
     global NXX
     if args.nxx:
         NXX = tuple(int(x) for x in args.nxx.split(","))
+    # Every reference run in this process (reference arm, CPU baseline, reference diagnostics
+    # and checkpoint timings) uses one OpenMP thread per physical core, bound close.
+    set_reference_threads()
     if args.impl == "reference":
         return run_reference(args)
     if args.diff_only:
@@ -319,18 +374,17 @@ def main():
         cpu = None
         if not args.no_cpu_baseline:
             try:
-                cpu = cpu_reference_rate(3, 1, 25.0, args.seed)
+                cpu = cpu_reference_rate(3, 2, 3, args.seed)
             except Exception as e:  # noqa: BLE001
                 cpu = {"unavailable": str(e)}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (Brill-Lindquist initial data, seeded)",
-            "config": {"workload": workload_name(),
-                       "interior_points": pts, "mode": "fused stages" if args.mode == 1 else "reference stage order",
-                       "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",
-                       "parallelism": f"replicas x{world}", "seed": args.seed, "bl": [m1, z1, m2, z2],
-                       "dt": grid_dt, "H_L2_last": h_hist[-1] if h_hist else None},
+            "config": bench_config(args.seed, world),
+            "mode": "fused stages" if args.mode == 1 else "reference stage order",
+            "l2": "inputs larger than L2 (5 state buffers x 246 MB), no flush",
+            "dt": grid_dt, "H_L2_last": h_hist[-1] if h_hist else None,
             "roofline": {"bound": "hbm", "kernel": "rhs_fused_kernel, all output groups (one interior RK stage: RHS + RK4 update + projection)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind,
@@ -505,7 +559,7 @@ def run_diagnostics(grid, args, reps: int = 3):
                     finally:
                         os.chdir(cwd)
                 rg.close()
-                res["reference_cores"] = os.cpu_count()
+                res["reference_cores"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
         except Exception as e:  # noqa: BLE001
             res["reference_unavailable"] = str(e)
     return res
@@ -571,7 +625,7 @@ def run_checkpoint(grid, args, reps: int = 3):
                     finally:
                         os.chdir(cwd)
                 rg.close()
-                res["reference_cores"] = os.cpu_count()
+                res["reference_cores"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
         except Exception as e:  # noqa: BLE001
             res["reference_unavailable"] = str(e)
     return res

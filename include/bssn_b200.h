@@ -331,16 +331,18 @@ int bssn_b200_constraint_integrals(const params_struct *params, const rfm_struct
                                    const REAL *diagnostic_gfs, double out[4], void *stream);
 
 /* The same integrals for callers that cannot allocate device memory -- code inside a host
- * framework that owns every allocation through its own pool or arena, code called while
- * a CUDA graph is being captured, or embedded hosts that forbid allocation after start-up.
+ * framework that owns every allocation through its own pool or arena (a cudaMalloc behind
+ * its back escapes its accounting and its memory cap), or embedded hosts that forbid
+ * allocation after start-up so that their footprint stays fixed.
  * No counterpart in the reference (whose integrals run on the host). It allocates
  * nothing: its partial sums live in a file-scope __device__ array of 16384*4+4 doubles
  * (512 KiB + 32 B), which every GPU that loads the library holds until the process exits.
  * Limit: grids of at most 33,554,432 interior points; larger grids return BSSN_B200_EINVAL.
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress)
- * with that device current; make that first call before any stream capture. All calls
- * share the one array, so calls that overlap on the GPU (other streams, other host
- * threads) race; every call overwrites the entries it reads, so nothing needs clearing.
+ * with that device current and keeps it; make that first call before any stream capture,
+ * and do not use the library across a cudaDeviceReset, which makes the kept address stale.
+ * All calls share the one array, so calls that overlap on the GPU (other streams, other
+ * host threads) race; every call overwrites the entries it reads, so nothing needs clearing.
  * Synchronises `stream`; `out` is a HOST array of 4 doubles. */
 int bssn_b200_constraint_integrals_noalloc(const params_struct *params, const rfm_struct *rfmstruct,
                                            const REAL *diagnostic_gfs, double out[4], void *stream);

@@ -324,7 +324,8 @@ def generate_adjoint(tag: str) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("NRPY_REFERENCE", str(ROOT.parent / "reference")),
+                    help="the nrpy checkout (default: $NRPY_REFERENCE, else ../reference beside this repository)")
     ap.add_argument("--variants", default=",".join(VARIANTS))
     ap.add_argument("--adjoint", default=",".join(ADJOINT_VARIANTS))
     ap.add_argument("--fd-order", type=int, default=4,

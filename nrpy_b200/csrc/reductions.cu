@@ -94,8 +94,9 @@ size_t constraint_integrals_scratch_doubles() { return (size_t)kRedBlocks * kRed
 // ---------------------------------------------------------------- allocation-free variant
 // Same integrals, for callers that must not allocate device memory: code running inside
 // a host framework that owns every allocation (a memory pool or arena that a foreign
-// cudaMalloc would bypass), code driven from a CUDA-graph-capture region, or embedded
-// hosts that forbid allocation after start-up. The partial sums live in a file-scope
+// cudaMalloc would bypass, breaking its accounting and its memory cap), or embedded hosts
+// that forbid allocation after start-up so that the footprint stays fixed. The call itself
+// allocates nothing. The partial sums live in a file-scope
 // __device__ array instead: one partial per block of kNoAllocPtsPerBlock interior points,
 // at most kNoAllocMaxBlocks blocks, i.e. grids of up to
 // kNoAllocMaxBlocks * kNoAllocPtsPerBlock = 33,554,432 interior points (512 KiB + 32 B of
@@ -150,7 +151,10 @@ __global__ void __launch_bounds__(kNoAllocThreads) constraint_partials_blocked_k
 
 long long constraint_integrals_noalloc_max_points() { return (long long)kNoAllocMaxBlocks * kNoAllocPtsPerBlock; }
 
-// Device address of g_noalloc_scratch, looked up once per device with that device current.
+// Device address of g_noalloc_scratch, looked up once per device with that device current
+// and kept for the life of the process: after a cudaDeviceReset (or any other teardown of
+// the device's primary context) the kept address is stale, so the library must not be used
+// across one.
 static double *noalloc_scratch_address(int *rc) {
   static std::mutex mu;
   static double *addr[64] = {nullptr};

@@ -111,7 +111,8 @@ def compile_variant(variant: str, proj: pathlib.Path, jobs: int) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--variants", default=",".join(VARIANTS))
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("NRPY_REFERENCE", str(HERE.parent.parent / "reference")),
+                    help="the nrpy checkout (default: $NRPY_REFERENCE, else ../reference beside this repository)")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     args = ap.parse_args()
     reference = pathlib.Path(args.reference)

@@ -2,7 +2,8 @@
 
 Runs nrpy.finite_difference.compute_fdcoeffs_fdstencl (nrpy/finite_difference.py:202-330)
 for the 4th-order operators on the hot path. Needs the reference importable, e.g.
-  PYTHONPATH=oracle/_ref/shim:/root/reference python tests/golden/make_fd_coeffs.py
+  PYTHONPATH=oracle/_ref/shim:$NRPY_REFERENCE python tests/golden/make_fd_coeffs.py
+($NRPY_REFERENCE: the nrpy checkout)
 (oracle/gen_ref.py writes the import shims under oracle/_ref/shim).
 """
 
