@@ -152,6 +152,8 @@ def host_cpu():
                 k, v = line.split(":", 1)
                 kv[k.strip()] = v.strip()
         info["model"] = kv.get("Model name")
+        info["lscpu"] = {k: kv[k] for k in ("CPU(s)", "Thread(s) per core", "Core(s) per socket", "Socket(s)",
+                                            "NUMA node(s)") if k in kv}
         cps, sock = int(kv.get("Core(s) per socket", "0")), int(kv.get("Socket(s)", "1") or 1)
         info["threads_per_core"] = int(kv.get("Thread(s) per core", "1") or 1)
         if cps > 0:
@@ -176,12 +178,21 @@ def host_cpu():
 
 
 def set_reference_threads():
-    """OpenMP settings of the reference's CPU runs: one thread per physical core, bound close
-    (set before the reference library is loaded, which reads them at start-up)."""
+    """OpenMP settings of the reference's CPU runs: one thread per physical core, bound close.
+    Set in the environment before the reference library is loaded, and through the OpenMP
+    runtime the reference library links (libgomp.so.1) in case it is already initialised;
+    `omp_max_threads` is what that runtime then reports."""
     cpu = host_cpu()
-    os.environ["OMP_NUM_THREADS"] = str(cpu["physical_cores"])
+    n = int(cpu["physical_cores"])
+    os.environ["OMP_NUM_THREADS"] = str(n)
     os.environ["OMP_PROC_BIND"] = "close"
     os.environ["OMP_PLACES"] = "cores"
+    try:
+        gomp = C.CDLL("libgomp.so.1")
+        gomp.omp_set_num_threads(n)
+        cpu["omp_max_threads"] = int(gomp.omp_get_max_threads())
+    except OSError:
+        cpu["omp_max_threads"] = None
     return cpu
 
 
@@ -206,14 +217,15 @@ def cpu_reference_rate(steps: int, warmup: int, runs: int, seed: int):
     rg.close()
     dt = float(np.median(times))
     pts = NXX[0] * NXX[1] * NXX[2]
-    return {"value": pts * steps / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
+    return {"value": pts * steps / dt, "unit": UNIT, "cores": cpu.get("omp_max_threads") or int(os.environ["OMP_NUM_THREADS"]),
             "kind": "reference",
             "sample": f"median of {runs} runs of {steps} RK4 steps of the full {NXX[0]}x{NXX[1]}x{NXX[2]} "
                       f"SinhSpherical grid after {warmup} warm-up steps (reference generated OpenMP C, fd_order "
                       f"{FD_ORDER}, MoL_step_forward_in_time incl. BCs + detgammabar; OMP_NUM_THREADS = physical "
                       f"cores, OMP_PROC_BIND=close)",
             "s_per_step": dt / steps, "run_s": times, "cpu_model": cpu.get("model"),
-            "physical_cores": cpu.get("physical_cores"), "logical_cpus": cpu.get("logical_cpus")}
+            "physical_cores": cpu.get("physical_cores"), "logical_cpus": cpu.get("logical_cpus"),
+            "lscpu": cpu.get("lscpu")}
 
 
 def workload_name() -> str:
@@ -265,6 +277,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=100)
     ap.add_argument("--no-diff", action="store_true", help="skip the adjoint-gradient section")
     ap.add_argument("--no-diag", action="store_true", help="skip the diagnostics-output section")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own CUDA build")
     ap.add_argument("--diff-only", action="store_true",
                     help="run only the adjoint-gradient section (one GPU) and print it as JSON (profiling)")
     ap.add_argument("--nxx", default=None, help="override the grid, e.g. 256,64,32 (profiling only)")
@@ -356,6 +369,14 @@ def main():
                 "flop_per_point": RHS_FLOP_PER_PT_STAGE[FD_ORDER],
                 "peak_source": "measured: independent FP64 FMA chains on every SM (bssn_b200_fp64_fma_rate)"}
 
+    # ---------------- baseline leg: the reference's own CUDA build on this GPU, same state
+    ref_gpu = None
+    if rank == 0 and not args.no_ref_gpu:
+        try:
+            ref_gpu = run_reference_gpu(grid, args, y0, value / world)
+        except Exception as e:  # noqa: BLE001
+            ref_gpu = {"unavailable": str(e)}
+
     # ---------------- end-to-end through the public API with host buffers
     e2e = None if args.no_e2e else run_e2e(grid, args, y0)
     diag = None if (args.no_diag or rank != 0) else run_diagnostics(grid, args)
@@ -399,6 +420,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "mixed": mixed,
             "batched": batched,
             "differentiation": differentiation,
@@ -409,6 +431,52 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_reference_gpu(grid, args, y0, our_value):
+    """Baseline leg: the reference's own GPU step (nrpy --cuda, its generated
+    MoL_step_forward_in_time compiled for sm_100a; oracle/_ref/sinh3d_cuda) on the same grid
+    and initial state, timed with CUDA events on its stream over the same number of RK4 steps
+    after 3 warm-up steps; one step from the shared state is first compared with this
+    library's step (per-gridfunction relative L2), so the timed code is known to compute the
+    same evolution."""
+    import torch
+
+    from oracle import ref
+
+    if not ref.cuda_available("sinh3d_cuda") or FD_ORDER != 4:
+        return {"unavailable": "oracle/_ref/sinh3d_cuda not built (python oracle/gen_ref.py --variants sinh3d_cuda)"}
+    m1, z1, m2, z2 = bl_params(args.seed)
+    y_host = y0.cpu().numpy()
+    rc = ref.RefCudaGrid(NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2)
+    try:
+        rc.set_y_n(y_host)
+        rc.steps(1)
+        y_ref = rc.y_n().reshape(24, -1)
+        grid.y_n.copy_(y0)
+        grid.MoL_step_forward_in_time(mode=args.mode)
+        torch.cuda.synchronize()
+        mine = grid.y_n.view(24, -1).cpu().numpy()
+        num = np.sqrt(((mine - y_ref) ** 2).sum(axis=1))
+        den = np.sqrt((y_ref**2).sum(axis=1))
+        # gridfunctions that vanish analytically (phi components; holes on the z axis) hold
+        # rounding noise only and are measured against the largest gridfunction's norm
+        rel = num / np.where(den < 1e-8 * den.max(), den.max(), den)
+        grid.y_n.copy_(y0)
+        rc.set_y_n(y_host)
+        rc.steps(3)  # warm-up
+        rc.set_y_n(y_host)
+        ms = rc.steps(args.steps)
+    finally:
+        rc.close()
+    pts = NXX[0] * NXX[1] * NXX[2]
+    v = pts * args.steps / (ms * 1e-3)
+    return {"value": v, "unit": UNIT, "ms_per_step": ms / args.steps, "steps": args.steps,
+            "speedup_of_this_library": our_value / v,
+            "one_step_rel_l2_vs_this_library_max": float(rel.max()),
+            "what": "the reference's generated CUDA (nrpy --cuda: Ricci_eval, rhs_eval, BCs, rk_substep_*, "
+                    "enforce_detgammabar kernels) compiled with nvcc -O2 -arch=sm_100a -rdc=true, timed with "
+                    "CUDA events around its MoL_step_forward_in_time calls"}
 
 
 def run_mixed(grid, args, y0, y_fp64, h_fp64, stream):

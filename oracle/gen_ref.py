@@ -23,8 +23,14 @@ Variants
   sph3dck: sph3d plus write_checkpoint/read_checkpoint (checkpoint file parity)
   sph3d8, sinh3d8, sphaxi8: sph3d, sinh3d and sphaxi with 8th-order finite differences
            (NGHOSTS = 5)
+  sinh3d_cuda: sinh3d emitted by the reference's CUDA path (``--cuda``), compiled with nvcc
+           for sm_100a (relocatable device code, the generated Makefile's flags with
+           ``-arch=sm_100a``) together with ``oracle/ref_harness_cuda.cu`` into
+           ``oracle/_ref/sinh3d_cuda/libref_cuda.so``: the reference's own GPU step, timed
+           beside this library's on the B200 (not part of the default variant list; it needs
+           nvcc, not a GPU, to build)
 
-Usage: python oracle/gen_ref.py [--variants sphaxi,sph3d,sinh3d] [--reference DIR]
+Usage: python oracle/gen_ref.py [--variants sphaxi,sph3d,sinh3d,sinh3d_cuda] [--reference DIR]
 """
 
 import argparse
@@ -45,6 +51,10 @@ VARIANTS = {
     "sph3d8": ["--coord", "Spherical", "--fd-order", "8"],
     "sinh3d8": ["--coord", "SinhSpherical", "--fd-order", "8"],
     "sphaxi8": ["--coord", "Spherical", "--axisym", "--fd-order", "8"],
+}
+# Variants emitted by the reference's CUDA path (built with nvcc; not in the default list).
+CUDA_VARIANTS = {
+    "sinh3d_cuda": ["--coord", "SinhSpherical", "--cuda"],
 }
 # Extra compiler definitions of a variant's harness build.
 HARNESS_DEFS = {"sph3dck": ["-DREF_HAS_CHECKPOINT"]}
@@ -77,7 +87,7 @@ def generate(variant: str, reference: pathlib.Path, shim: pathlib.Path) -> pathl
     env = dict(os.environ)
     env["PYTHONPATH"] = f"{shim}:{reference}"
     env["PATH"] = f"{shim / 'bin'}:{env.get('PATH', '')}"
-    cmd = [sys.executable, str(HERE / "ref_project.py"), "--project-dir", str(proj)] + VARIANTS[variant]
+    cmd = [sys.executable, str(HERE / "ref_project.py"), "--project-dir", str(proj)] + {**VARIANTS, **CUDA_VARIANTS}[variant]
     with open(vdir / "generate.log", "w") as log:
         subprocess.run(cmd, cwd=vdir, env=env, stdout=log, stderr=subprocess.STDOUT, check=True)
     return proj
@@ -108,6 +118,35 @@ def compile_variant(variant: str, proj: pathlib.Path, jobs: int) -> None:
         print(f"built {lib}")
 
 
+def compile_cuda_variant(variant: str, proj: pathlib.Path, jobs: int) -> None:
+    """nvcc build of a CUDA project: every generated .cu (not main.cu) with the generated
+    Makefile's NVCCFLAGS for sm_100a, its .cc files with the host compiler, and the CUDA
+    harness, linked into one shared library (device link included)."""
+    vdir = REF_OUT / variant
+    objdir = vdir / "obj_cuda"
+    objdir.mkdir(exist_ok=True)
+    cu = sorted(p for p in proj.rglob("*.cu") if p.name != "main.cu") + [HERE / "ref_harness_cuda.cu"]
+    cc = sorted(proj.rglob("*.cc"))
+    nv = ["nvcc", "-O2", "-arch=sm_100a", "--relocatable-device-code=true", "-allow-unsupported-compiler",
+          "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp", "-Xcompiler", "-march=x86-64-v3", "-w", f"-I{proj}"]
+    cxx = ["g++", "-O2", "-fPIC", "-fopenmp", "-march=x86-64-v3", "-w", f"-I{proj}", "-I/usr/local/cuda/include"]
+
+    def one(src: pathlib.Path) -> pathlib.Path:
+        rel = src.relative_to(proj) if proj in src.parents else pathlib.Path(src.name)
+        obj = objdir / (str(rel).replace("/", "__") + ".o")
+        base = nv if src.suffix == ".cu" else cxx
+        subprocess.run(base + ["-c", str(src), "-o", str(obj)], check=True)
+        return obj
+
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        objs = list(ex.map(one, cu + cc))
+    lib = vdir / "libref_cuda.so"
+    subprocess.run(["nvcc", "-shared", "-arch=sm_100a", "--relocatable-device-code=true", "-Xcompiler", "-fopenmp",
+                    "-o", str(lib)] + [str(o) for o in objs] + ["-lm"], check=True)
+    shutil.rmtree(objdir)
+    print(f"built {lib}")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--variants", default=",".join(VARIANTS))
@@ -122,7 +161,10 @@ def main() -> None:
     write_shims(shim)
     for v in args.variants.split(","):
         proj = generate(v, reference, shim)
-        compile_variant(v, proj, args.jobs)
+        if v in CUDA_VARIANTS:
+            compile_cuda_variant(v, proj, args.jobs)
+        else:
+            compile_variant(v, proj, args.jobs)
 
 
 if __name__ == "__main__":

@@ -267,6 +267,78 @@ class RefGrid:
         return inner, outer
 
 
+def cuda_available(variant: str = "sinh3d_cuda") -> bool:
+    return (REF_DIR / variant / "libref_cuda.so").exists()
+
+
+_CUDA_LIBS = {}
+
+
+def _load_cuda(variant: str) -> C.CDLL:
+    if variant in _CUDA_LIBS:
+        return _CUDA_LIBS[variant]
+    p = REF_DIR / variant / "libref_cuda.so"
+    if not p.exists():
+        raise FileNotFoundError(f"reference CUDA library {p} missing; run `python oracle/gen_ref.py --variants {variant}`")
+    lib = C.CDLL(str(p))
+    vp, ip, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
+    lib.refc_create.restype = vp
+    lib.refc_create.argtypes = [ip, ip, ip] + [C.c_double] * 7
+    lib.refc_N.argtypes = [vp, ip]
+    lib.refc_dt.restype = C.c_double
+    lib.refc_dt.argtypes = [vp]
+    lib.refc_nn.argtypes = [vp]
+    lib.refc_set_y_n.argtypes = [vp, dp]
+    lib.refc_get_y_n.argtypes = [vp, dp]
+    lib.refc_steps.restype = C.c_double
+    lib.refc_steps.argtypes = [vp, ip]
+    lib.refc_destroy.argtypes = [vp]
+    _CUDA_LIBS[variant] = lib
+    return lib
+
+
+class RefCudaGrid:
+    """One SinhSpherical grid of the reference's own CUDA build (nrpy --cuda, sm_100a): set up
+    as its generated main() and numerical_grids_and_timestep() do, stepped by its generated
+    MoL_step_forward_in_time on the current GPU."""
+
+    def __init__(self, Nxx, grid_physical_size: float, SINHW: float = 0.2, BH1_mass: float = 0.5,
+                 BH1_posn_z: float = 0.5, BH2_mass: float = 0.5, BH2_posn_z: float = -0.5, CFL_FACTOR: float = 0.5,
+                 variant: str = "sinh3d_cuda"):
+        self.lib = _load_cuda(variant)
+        self.h = self.lib.refc_create(int(Nxx[0]), int(Nxx[1]), int(Nxx[2]), grid_physical_size, SINHW, BH1_mass,
+                                      BH1_posn_z, BH2_mass, BH2_posn_z, CFL_FACTOR)
+        self.N = tuple(self.lib.refc_N(self.h, d) for d in range(3))
+        self.ntot = self.N[0] * self.N[1] * self.N[2]
+
+    @property
+    def dt(self) -> float:
+        return self.lib.refc_dt(self.h)
+
+    def y_n(self) -> np.ndarray:
+        out = np.zeros(NUM_EVOL_GFS * self.ntot)
+        if self.lib.refc_get_y_n(self.h, _dp(out)) != 0:
+            raise RuntimeError("reference CUDA build: device-to-host copy failed")
+        return out
+
+    def set_y_n(self, y: np.ndarray) -> None:
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        if self.lib.refc_set_y_n(self.h, _dp(y)) != 0:
+            raise RuntimeError("reference CUDA build: host-to-device copy failed")
+
+    def steps(self, n: int) -> float:
+        """n generated MoL_step_forward_in_time calls; device milliseconds (CUDA events)."""
+        ms = self.lib.refc_steps(self.h, int(n))
+        if ms < 0:
+            raise RuntimeError("reference CUDA build: a CUDA error occurred during the steps")
+        return ms
+
+    def close(self):
+        if self.h:
+            self.lib.refc_destroy(self.h)
+            self.h = None
+
+
 def struct_layout(variant: str) -> dict:
     lib = _load(variant)
     names = ["sizeof_commondata", "sizeof_params", "sizeof_bc_struct", "sizeof_griddata", "sizeof_innerpt",
