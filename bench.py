@@ -140,9 +140,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+_HOST_CPU = None
+
+
 def host_cpu():
     """The host CPU as lscpu reports it: model, physical cores (cores per socket x sockets,
-    capped by this process's CPU affinity) and logical CPUs."""
+    capped by this process's CPU affinity) and logical CPUs. Evaluated once, at the first
+    call: an OpenMP runtime with OMP_PROC_BIND set later binds the main thread to one core,
+    which would shrink the affinity seen afterwards."""
+    global _HOST_CPU
+    if _HOST_CPU is not None:
+        return dict(_HOST_CPU)
     info = {"model": None, "physical_cores": None, "logical_cpus": os.cpu_count()}
     try:
         out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
@@ -174,6 +182,7 @@ def host_cpu():
         info["physical_cores"] = max(1, min(info["physical_cores"], aff // tpc if aff >= tpc else aff))
     except (AttributeError, OSError):
         pass
+    _HOST_CPU = dict(info)
     return info
 
 

@@ -41,10 +41,11 @@ def available(variant: str) -> bool:
 _LIBS = {}
 
 
-def _load(variant: str) -> C.CDLL:
-    if variant in _LIBS:
-        return _LIBS[variant]
-    p = lib_path(variant)
+def _load(variant: str, isa: str = None) -> C.CDLL:
+    key = (variant, isa or cpu_isa())
+    if key in _LIBS:
+        return _LIBS[key]
+    p = lib_path(variant, isa)
     if not p.exists():
         raise FileNotFoundError(f"oracle library {p} missing; run `python oracle/gen_ref.py`")
     lib = C.CDLL(str(p))
@@ -104,7 +105,7 @@ def _load(variant: str) -> C.CDLL:
               "ref_offsetof_commondata_bc", "ref_offsetof_commondata_nn"):
         getattr(lib, f).restype = C.c_size_t
         getattr(lib, f).argtypes = []
-    _LIBS[variant] = lib
+    _LIBS[key] = lib
     return lib
 
 
@@ -114,13 +115,19 @@ def _dp(a: np.ndarray):
 
 
 class RefGrid:
-    """One grid of the reference project: set-up exactly as its generated main()."""
+    """One grid of the reference project: set-up exactly as its generated main().
+
+    ``isa`` picks the build ("avx512" or "avx2"; default: the host's best). The reference's
+    loops over i0 advance by the SIMD width and write whole vectors: with AVX-512 (8 doubles)
+    the last vector of a row runs 4 points past its interior end when Nxx0 = 1 (mod 8), into
+    the first interior point of the next row, which another OpenMP thread may already have
+    written. The AVX2 build (4 doubles) never runs past the end of a row."""
 
     def __init__(self, variant: str, Nxx, grid_physical_size: float, SINHW: float = 0.2, BH1_mass: float = 0.5,
                  BH1_posn_z: float = 0.5, BH2_mass: float = 0.5, BH2_posn_z: float = -0.5, CFL_FACTOR: float = 0.5,
-                 outer_bc_type: str = "radiation"):
+                 outer_bc_type: str = "radiation", isa: str = None):
         self.variant = variant
-        self.lib = _load(variant)
+        self.lib = _load(variant, isa)
         self.h = self.lib.ref_create(int(Nxx[0]), int(Nxx[1]), int(Nxx[2]), grid_physical_size, SINHW, BH1_mass,
                                      BH1_posn_z, BH2_mass, BH2_posn_z, CFL_FACTOR,
                                      1 if outer_bc_type == "extrapolation" else 0)
