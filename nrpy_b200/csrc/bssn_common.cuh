@@ -105,9 +105,6 @@ struct StageBuffers {
   double *kin;   // stage input
   double *kout;  // RHS / stage output buffer
 };
-// Whether fused stages evaluate Ricci_eval inside the RHS kernel (then the stage launches no
-// Ricci kernels of its own).
-bool fuse_ricci();
 int launch_rhs_fused_stage(Variant v, bool mixed, int stage, double dt, const GridDims &g, const RfmArrays &rfm,
                            const PhysParams &pp, const double *aux, const StageBuffers &b, double *krhs,
                            cudaStream_t s);

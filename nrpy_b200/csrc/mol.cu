@@ -109,7 +109,7 @@ int mol_stage(const commondata_struct *cd, griddata_struct *gd, int grid, int st
   const bool radiation = outer_is(cd, "radiation");
   const bool extrap = outer_is(cd, "extrapolation");
   // In the stage-4 RK update the reference writes y_n in place; OUT is y_n then.
-  if (mode == 0 || !fuse_ricci()) BSSN_TRY(launch_ricci(v, g, rfm, b.kin, G.gridfuncs.auxevol_gfs, s, mixed != 0));
+  BSSN_TRY(launch_ricci(v, g, rfm, b.kin, G.gridfuncs.auxevol_gfs, s, mixed != 0));
   if (mode == 0) {
     BSSN_TRY(launch_rhs(v, mixed != 0, g, rfm, pp, G.gridfuncs.auxevol_gfs, b.kin, b.kout, s));
     if (radiation) {

@@ -6,8 +6,6 @@
 // Layout: gf-major IDX4(gf,i0,i1,i2) = i0 + N0*(i1 + N1*(i2 + N2*gf)). One thread per
 // interior point; a warp spans 32 consecutive i0, so each stencil load of a warp touches
 // one or two contiguous 256-byte segments that neighbouring warps reuse from L1/L2.
-#include <cstdio>
-#include <cstdlib>
 #include <type_traits>
 
 #include "bssn_common.cuh"
@@ -176,50 +174,6 @@ static dim3 group_grid(const GridDims &g, int nt) {
   const int i2 = NGHOSTS + blockIdx.z * blockDim.z + threadIdx.z;       \
   if (i0 >= g.N0 - NGHOSTS || i1 >= g.N1 - NGHOSTS || i2 >= g.N2 - NGHOSTS) return;
 
-// Plane order and L2 prefetch of the group kernels. The blocks of a launch are dispatched
-// in blockIdx order, so the resident blocks form a window of about two i2 planes that moves
-// along i2: each input line is first read, from DRAM, by the block at the window's leading
-// edge. rev = 1 walks the planes from the top down (a kernel that follows one walking upwards
-// then starts on the planes the previous kernel left in L2); pf > 0 lets every block, on
-// entry, ask L2 for its tile's rows of the plane pf planes ahead of it in its walk direction,
-// so that the leading edge finds them there.
-struct Sweep {
-  int rev;  // 0: i2 increasing with blockIdx.z; 1: decreasing
-  int pf;   // prefetch distance in planes (0: none)
-};
-
-__device__ __forceinline__ void l2_prefetch(const double *p) {
-  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-}
-
-// L2 prefetch of this block's tile rows (blockDim.x points along i0, blockDim.y rows along i1)
-// of plane i2p for gridfunctions gfs[0..ngf) of `base`; every address is clamped into the grid.
-__device__ __forceinline__ void prefetch_tile_rows(const GridDims &g, const double *base, const int *gfs, int ngf,
-                                                   int i2p) {
-  if (i2p < 0 || i2p >= g.N2) return;
-  const int i0a = NGHOSTS + blockIdx.x * blockDim.x;
-  const int i1a = NGHOSTS + blockIdx.y * blockDim.y;
-  const int rows = blockDim.y, lines = (int)(blockDim.x * sizeof(double) + 127) / 128 + 1;
-  const int nthr = blockDim.x * blockDim.y * blockDim.z;
-  const int t = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
-  for (int j = t; j < ngf * rows * lines; j += nthr) {
-    const int l = j % lines, r = (j / lines) % rows, k = j / (lines * rows);
-    const int i1 = min(i1a + r, g.N1 - 1), i0 = min(i0a + 16 * l, g.N0 - 1);
-    l2_prefetch(base + (size_t)gfs[k] * g.ntot + (size_t)i2p * g.s2 + (size_t)i1 * g.s1 + i0);
-  }
-}
-
-__constant__ int kPrefetchAllGfs[NUM_EVOL_GFS] = {0,  1,  2,  3,  4,  5,  6,  7,  8,  9,  10, 11,
-                                                 12, 13, 14, 15, 16, 17, 18, 19, 20, 21, 22, 23};
-// Ricci_eval reads hDD (11-16) and lambdaU (17-19).
-constexpr int kRicciGf0 = HDD00GF, kRicciNgf = 9;
-
-#define GROUP_INDEX_SWEEP_OR_RETURN(g, bz)                              \
-  const int i0 = NGHOSTS + blockIdx.x * blockDim.x + threadIdx.x;       \
-  const int i1 = NGHOSTS + blockIdx.y * blockDim.y + threadIdx.y;       \
-  const int i2 = NGHOSTS + (bz) * blockDim.z + threadIdx.z;             \
-  if (i0 >= g.N0 - NGHOSTS || i1 >= g.N1 - NGHOSTS || i2 >= g.N2 - NGHOSTS) return;
-
 template <typename T>
 __device__ __forceinline__ volatile T *thread_slots() {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -241,18 +195,9 @@ __device__ __forceinline__ void ricci_body(const GridDims &g, const RfmArrays &r
 
 template <Variant V, int G, typename T>
 __global__ void __launch_bounds__(RicciG<V, G>::NT, 1) ricci_kernel(const GridDims g, const RfmArrays rfm,
-                                                          const double *__restrict__ in, double *__restrict__ aux,
-                                                          const Sweep sw) {
+                                                          const double *__restrict__ in, double *__restrict__ aux) {
   volatile T *sm = thread_slots<T>();
-  const int bz = sw.rev ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z;
-  if (sw.pf) {
-    const int i2p = NGHOSTS + bz * (int)blockDim.z + (sw.rev ? -sw.pf : sw.pf + (int)blockDim.z - 1);
-    int gfs[kRicciNgf];
-#pragma unroll
-    for (int k = 0; k < kRicciNgf; k++) gfs[k] = kRicciGf0 + k;
-    for (int z = 0; z < (int)blockDim.z; z++) prefetch_tile_rows(g, in, gfs, kRicciNgf, i2p + (sw.rev ? -z : z));
-  }
-  GROUP_INDEX_SWEEP_OR_RETURN(g, bz);
+  GROUP_INDEX_OR_RETURN(g);
   ricci_body<V, G, T, RicciG<V, G>::NT>(g, rfm, in, aux, i0, i1, i2, sm);
 }
 
@@ -362,19 +307,12 @@ __device__ __forceinline__ void rk_and_project_point(const GridDims &g, const Rf
 // of that group's gridfunctions; the group holding hDD also applies the detgammabar
 // projection to the new hDD. The raw RHS is also stored to `krhs` on the interior shell
 // (the layer next to each face), where the outer radiation condition reads it.
-// R_ij written earlier by the same thread (the Ricci phases of rhs_ricci_fused_kernel): read
-// through L2 (ld.global.cg), not the read-only path, which may hold an older copy of the line.
-struct OwnAuxCtx : PointCtx {
-  __device__ __forceinline__ double ldaux(int k) const { return __ldcg(aux + k * ntot); }
-};
-
-template <Variant V, typename T, int STAGE, int G, int NTB, typename S, typename Ctx = PointCtx>
+template <Variant V, typename T, int STAGE, int G, int NTB, typename S>
 __device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
                                            const double *aux, const StageBuffers &b, double *krhs, const double dt,
                                            int i0, int i1, int i2, S *sm) {
   using Grp = RhsG<V, G>;
-  Ctx ctx;
-  static_cast<PointCtx &>(ctx) = make_ctx(g, rfm, b.kin, aux, i0, i1, i2);
+  PointCtx ctx = make_ctx(g, rfm, b.kin, aux, i0, i1, i2);
   ctx.eta = pp.eta;
   ctx.KreissOliger_strength_gauge = pp.ko_gauge;
   ctx.KreissOliger_strength_nongauge = pp.ko_nongauge;
@@ -416,64 +354,10 @@ __device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &r
 template <Variant V, typename T, int STAGE, int G>
 __global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp,
                                                               const double *__restrict__ aux, const StageBuffers b,
-                                                              double *__restrict__ krhs, const double dt,
-                                                              const Sweep sw) {
-  using Grp = RhsG<V, G>;
+                                                              double *__restrict__ krhs, const double dt) {
   volatile T *sm = thread_slots<T>();
-  const int bz = sw.rev ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z;
-  if (sw.pf) {
-    // the stage input ahead of the walk; this tile's RK operands (y, running total) and
-    // R_ij of its own plane, read in the epilogue and by the algebra
-    const int i2a = NGHOSTS + bz * (int)blockDim.z;
-    const int i2p = i2a + (sw.rev ? -sw.pf : sw.pf + (int)blockDim.z - 1);
-    for (int z = 0; z < (int)blockDim.z; z++) {
-      prefetch_tile_rows(g, b.kin, kPrefetchAllGfs, NUM_EVOL_GFS, i2p + (sw.rev ? -z : z));
-      int gfs[Grp::N];
-#pragma unroll
-      for (int k = 0; k < Grp::N; k++) gfs[k] = Grp::GF(k);
-      prefetch_tile_rows(g, b.y, gfs, Grp::N, i2a + z);
-      if (STAGE != 1) prefetch_tile_rows(g, b.run, gfs, Grp::N, i2a + z);
-      if (G == 0 && aux) {
-        int ag[NUM_AUXEVOL_GFS];
-#pragma unroll
-        for (int k = 0; k < NUM_AUXEVOL_GFS; k++) ag[k] = k;
-        prefetch_tile_rows(g, aux, ag, NUM_AUXEVOL_GFS, i2a + z);
-      }
-    }
-  }
-  GROUP_INDEX_SWEEP_OR_RETURN(g, bz);
+  GROUP_INDEX_OR_RETURN(g);
   fused_body<V, T, STAGE, G, RhsG<V, G>::NT>(g, rfm, pp, aux, b, krhs, dt, i0, i1, i2, sm);
-}
-
-// Ricci_eval and RHS output group 0 of one interior point in one launch: both Ricci output
-// groups run first (their R_ij go to aux, as Ricci_eval writes them), then the group that
-// reads R_ij, with the RK update and projection of fused_body. The phases run one after the
-// other in each thread and share its shared-memory slots.
-template <Variant V, typename T, int STAGE>
-__global__ void __launch_bounds__(RhsG<V, 0>::NT, 1)
-    rhs_ricci_fused_kernel(const GridDims g, const RfmArrays rfm, const PhysParams pp, double *__restrict__ aux,
-                           const StageBuffers b, double *__restrict__ krhs, const double dt, const Sweep sw) {
-  using Grp = RhsG<V, 0>;
-  constexpr int NT = Grp::NT;
-  static_assert(RicciG<V, 0>::NT == NT && RicciG<V, 1>::NT == NT, "one block size for every phase");
-  volatile T *sm = thread_slots<T>();
-  const int bz = sw.rev ? (int)(gridDim.z - 1 - blockIdx.z) : (int)blockIdx.z;
-  if (sw.pf) {
-    const int i2a = NGHOSTS + bz * (int)blockDim.z;
-    const int i2p = i2a + (sw.rev ? -sw.pf : sw.pf + (int)blockDim.z - 1);
-    for (int z = 0; z < (int)blockDim.z; z++) {
-      prefetch_tile_rows(g, b.kin, kPrefetchAllGfs, NUM_EVOL_GFS, i2p + (sw.rev ? -z : z));
-      int gfs[Grp::N];
-#pragma unroll
-      for (int k = 0; k < Grp::N; k++) gfs[k] = Grp::GF(k);
-      prefetch_tile_rows(g, b.y, gfs, Grp::N, i2a + z);
-      if (STAGE != 1) prefetch_tile_rows(g, b.run, gfs, Grp::N, i2a + z);
-    }
-  }
-  GROUP_INDEX_SWEEP_OR_RETURN(g, bz);
-  ricci_body<V, 0, T, NT>(g, rfm, b.kin, aux, i0, i1, i2, sm);
-  ricci_body<V, 1, T, NT>(g, rfm, b.kin, aux, i0, i1, i2, sm);
-  fused_body<V, T, STAGE, 0, NT, volatile T, OwnAuxCtx>(g, rfm, pp, aux, b, krhs, dt, i0, i1, i2, sm);
 }
 
 // RK update plus projection of listed boundary points whose RHS is already in krhs.
@@ -517,39 +401,12 @@ static int set_smem(KernelPtr k, size_t bytes) {
   return BSSN_B200_OK;
 }
 
-// Plane order and prefetch distance of the group kernels, in launch order within a stage
-// (Ricci groups, then RHS groups): alternate kernels walk the planes in opposite directions
-// and prefetch 4 planes ahead (measured at SinhSpherical 256x64x64 on a B200: 108.1 M
-// pt-updates/s with neither, 109.4 M alternating only, 112.1 M prefetching only, 113.0 M with
-// both; 8 planes ahead was slower). BSSN_B200_SWEEP=<alternate 0|1>,<prefetch planes>
-// overrides this for measurements.
-static Sweep sweep_of(int kernel_in_stage) {
-  static int serp = -1, pf = 4;
-  if (serp < 0) {
-    serp = 1;
-    if (const char *e = getenv("BSSN_B200_SWEEP")) sscanf(e, "%d,%d", &serp, &pf);
-  }
-  return Sweep{serp ? (kernel_in_stage & 1) : 0, pf};
-}
-
-// Whether a fused stage evaluates Ricci_eval inside the RHS group-0 kernel
-// (rhs_ricci_fused_kernel) instead of in launches of its own. BSSN_B200_FUSE_RICCI=0|1
-// overrides the default for measurements.
-bool fuse_ricci() {
-  static int f = -1;
-  if (f < 0) {
-    f = 0;
-    if (const char *e = getenv("BSSN_B200_FUSE_RICCI")) f = atoi(e) != 0;
-  }
-  return f != 0;
-}
-
 template <Variant V, int G, typename T>
 static int launch_ricci_group(const GridDims &g, const RfmArrays &rfm, const double *in, double *aux, cudaStream_t s) {
   using Grp = RicciG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(ricci_kernel<V, G, T>, sb));
-  ricci_kernel<V, G, T><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, in, aux, sweep_of(G));
+  ricci_kernel<V, G, T><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, in, aux);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -630,34 +487,8 @@ static int launch_fused_group(const GridDims &g, const RfmArrays &rfm, const Phy
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(rhs_fused_kernel<V, T, STAGE, G>, sb));
-  rhs_fused_kernel<V, T, STAGE, G><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(
-      g, rfm, pp, aux, b, krhs, dt, sweep_of(kRicciGroups + G));
-  BSSN_LAUNCH_CHECK();
-  return BSSN_B200_OK;
-}
-
-// With Ricci fused into the first RHS group: two launches per stage (Ricci + RHS group 0, then
-// RHS group 1), walking the planes in opposite directions.
-template <Variant V, typename T, int STAGE>
-static int launch_ricci_fused_stage_groups(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp,
-                                           double *aux, const StageBuffers &b, double *krhs, double dt,
-                                           cudaStream_t s) {
-  static_assert(kRhsGroups == 2, "Ricci fusion pairs the Ricci groups with RHS group 0 of two");
-  using G0 = RhsG<V, 0>;
-  using G1 = RhsG<V, 1>;
-  constexpr int slots = (G0::SLOTS > RicciG<V, 0>::SLOTS ? G0::SLOTS : RicciG<V, 0>::SLOTS) > RicciG<V, 1>::SLOTS
-                            ? (G0::SLOTS > RicciG<V, 0>::SLOTS ? G0::SLOTS : RicciG<V, 0>::SLOTS)
-                            : RicciG<V, 1>::SLOTS;
-  constexpr size_t sb = (size_t)slots * G0::NT * sizeof(T);
-  const Sweep sw0 = sweep_of(0), sw1 = sweep_of(1);
-  BSSN_TRY(set_smem(rhs_ricci_fused_kernel<V, T, STAGE>, sb));
-  rhs_ricci_fused_kernel<V, T, STAGE><<<group_grid(g, G0::NT), group_block(G0::NT), sb, s>>>(g, rfm, pp, aux, b, krhs,
-                                                                                             dt, sw0);
-  BSSN_LAUNCH_CHECK();
-  constexpr size_t sb1 = slot_bytes<G1, T>();
-  BSSN_TRY(set_smem(rhs_fused_kernel<V, T, STAGE, 1>, sb1));
-  rhs_fused_kernel<V, T, STAGE, 1><<<group_grid(g, G1::NT), group_block(G1::NT), sb1, s>>>(g, rfm, pp, aux, b, krhs,
-                                                                                           dt, sw1);
+  rhs_fused_kernel<V, T, STAGE, G><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, pp, aux, b,
+                                                                                              krhs, dt);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -665,8 +496,6 @@ static int launch_ricci_fused_stage_groups(const GridDims &g, const RfmArrays &r
 template <Variant V, typename T, int STAGE>
 static int launch_fused_stage_groups(const GridDims &g, const RfmArrays &rfm, const PhysParams &pp, const double *aux,
                                      const StageBuffers &b, double *krhs, double dt, cudaStream_t s) {
-  if (fuse_ricci())
-    return launch_ricci_fused_stage_groups<V, T, STAGE>(g, rfm, pp, const_cast<double *>(aux), b, krhs, dt, s);
   return for_each_group<0, kRhsGroups>(
       [&](auto gc) { return launch_fused_group<V, T, STAGE, decltype(gc)::value>(g, rfm, pp, aux, b, krhs, dt, s); });
 }
