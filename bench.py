@@ -289,6 +289,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own CUDA build")
     ap.add_argument("--diff-only", action="store_true",
                     help="run only the adjoint-gradient section (one GPU) and print it as JSON (profiling)")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched section (one GPU) and print it as JSON (profiling)")
     ap.add_argument("--nxx", default=None, help="override the grid, e.g. 256,64,32 (profiling only)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -302,6 +304,12 @@ def main():
         return run_reference(args)
     if args.diff_only:
         print(json.dumps(run_differentiation(fd_check=False)))
+        return None
+    if args.batched_only:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        print(json.dumps(run_batched(args, 1, 0, None)))
         return None
 
     import torch
@@ -361,6 +369,7 @@ def main():
     clocks = clk.summary()
 
     y_fp64 = grid.y_n.clone()
+    y0_host = y0.cpu().numpy() if rank == 0 else None
     mixed = None if args.no_mixed else run_mixed(grid, args, y0, y_fp64, h_hist, stream)
 
     # ---------------- dominant kernel alone: fused interior RHS + RK update, per stage
@@ -402,11 +411,17 @@ def main():
 
     if rank == 0:
         cpu = None
+        y_cmp = mixed.pop("_y_cmp", None) if mixed else None
         if not args.no_cpu_baseline:
             try:
                 cpu = cpu_reference_rate(3, 2, 3, args.seed)
             except Exception as e:  # noqa: BLE001
                 cpu = {"unavailable": str(e)}
+            if mixed is not None and y_cmp is not None:
+                try:
+                    mixed.update(mixed_vs_reference(y0_host, y_cmp, mixed["compare_steps"], args.seed))
+                except Exception as e:  # noqa: BLE001
+                    mixed["oracle_unavailable"] = str(e)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -430,6 +445,13 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
+            "mixed_value": mixed["value"] if mixed else None,
+            "mixed_H_L2": mixed.get("H_L2_at_compare") if mixed else None,
+            "mixed_H_L2_oracle": mixed.get("H_L2_oracle") if mixed else None,
+            "mixed_H_L2_fp64": mixed.get("H_L2_fp64_at_compare") if mixed else None,
+            "mixed_rel_l2_vs_oracle_max": mixed.get("rel_l2_vs_oracle_max") if mixed else None,
+            "mixed_compare_steps": mixed.get("compare_steps") if mixed else None,
+            "batched_value": batched["value"] if batched else None,
             "mixed": mixed,
             "batched": batched,
             "differentiation": differentiation,
@@ -440,6 +462,32 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def mixed_vs_reference(y0_host, y_mixed, steps, seed):
+    """The reference's generated C (host cores) advanced `steps` RK4 steps from the bench's
+    initial state: its H-constraint L2 (its Ricci_eval + constraints_eval, volume measure of
+    diagnostics_volume_integration) and the per-gridfunction relative L2 of the mixed run's
+    state against it (gridfunctions that vanish analytically, the phi components for holes on
+    the z axis, are measured against the largest gridfunction's norm)."""
+    from oracle import ref
+
+    m1, z1, m2, z2 = bl_params(seed)
+    rg = ref.RefGrid(SINH_VARIANT, NXX, AMPL, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2)
+    try:
+        rg.set_y_n(y0_host)
+        rg.step(steps)
+        yr = rg.y_n()
+        h = rg.h_l2(yr)
+    finally:
+        rg.close()
+    r = yr.reshape(24, -1)
+    m = y_mixed.reshape(24, -1)
+    num = np.sqrt(((m - r) ** 2).sum(axis=1))
+    den = np.sqrt((r**2).sum(axis=1))
+    rel = num / np.where(den < 1e-8 * den.max(), den.max(), den)
+    return {"H_L2_oracle": h, "rel_l2_vs_oracle_max": float(rel.max()),
+            "rel_l2_vs_oracle_per_gf": [float(x) for x in rel]}
 
 
 def run_reference_gpu(grid, args, y0, our_value):
@@ -468,9 +516,9 @@ def run_reference_gpu(grid, args, y0, our_value):
         mine = grid.y_n.view(24, -1).cpu().numpy()
         num = np.sqrt(((mine - y_ref) ** 2).sum(axis=1))
         den = np.sqrt((y_ref**2).sum(axis=1))
-        # gridfunctions that vanish analytically (phi components; holes on the z axis) hold
-        # rounding noise only and are measured against the largest gridfunction's norm
-        rel = num / np.where(den < 1e-8 * den.max(), den.max(), den)
+        # each gridfunction's difference against the largest gridfunction's norm (several
+        # components start at zero and hold rounding-size values after one step)
+        rel = num / den.max()
         grid.y_n.copy_(y0)
         rc.set_y_n(y_host)
         rc.steps(3)  # warm-up
@@ -482,16 +530,26 @@ def run_reference_gpu(grid, args, y0, our_value):
     v = pts * args.steps / (ms * 1e-3)
     return {"value": v, "unit": UNIT, "ms_per_step": ms / args.steps, "steps": args.steps,
             "speedup_of_this_library": our_value / v,
-            "one_step_rel_l2_vs_this_library_max": float(rel.max()),
+            "one_step_l2_diff_vs_this_library_max": float(rel.max()),
+            "one_step_l2_diff_measure": "max over gridfunctions of ||reference GPU - this library|| / ||largest gridfunction||",
             "what": "the reference's generated CUDA (nrpy --cuda: Ricci_eval, rhs_eval, BCs, rk_substep_*, "
                     "enforce_detgammabar kernels) compiled with nvcc -O2 -arch=sm_100a -rdc=true, timed with "
                     "CUDA events around its MoL_step_forward_in_time calls"}
 
 
+def oracle_steps(steps: int) -> int:
+    """Steps at which the mixed run is compared with the reference on the host: the run's
+    length capped at 40 (the reference takes about 0.2 s per step of this grid on 16 cores),
+    a multiple of the H-constraint cadence."""
+    return max(H_EVERY, (min(steps, 40) // H_EVERY) * H_EVERY)
+
+
 def run_mixed(grid, args, y0, y_fp64, h_fp64, stream):
     """Same workload with the Ricci/RHS algebra in FP32 (stencils, state, RK accumulation,
     detgammabar projection and constraint reductions in FP64): rate, H-constraint L2 next
-    to the FP64 run's, and the per-gridfunction relative L2 of the final state vs FP64."""
+    to the FP64 run's, and the per-gridfunction relative L2 of the final state vs FP64. The
+    state after oracle_steps() steps is kept (host copy) for the comparison with the
+    reference."""
     import torch
 
     grid.free_stepper()
@@ -516,6 +574,13 @@ def run_mixed(grid, args, y0, y_fp64, h_fp64, stream):
         b.record(st)
     b.synchronize()
     ms = a.elapsed_time(b)
+    # untimed: the mixed state at the step count compared with the reference
+    ncmp = oracle_steps(args.steps)
+    grid.y_n.copy_(y0)
+    with torch.cuda.stream(st):
+        grid.run_stepper(ncmp)
+    torch.cuda.synchronize()
+    y_cmp = grid.y_n.cpu().numpy()
     m = grid.y_n.view(24, -1)
     f = y_fp64.view(24, -1)
     num = torch.linalg.vector_norm(m - f, dim=1)
@@ -524,6 +589,8 @@ def run_mixed(grid, args, y0, y_fp64, h_fp64, stream):
     nz = (torch.linalg.vector_norm(f, dim=1) > 1e-12 * torch.linalg.vector_norm(f, dim=1).max()).cpu().numpy()
     grid.free_stepper()
     return {"value": grid.n_interior * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "_y_cmp": y_cmp, "compare_steps": ncmp, "H_L2_at_compare": h[ncmp // H_EVERY - 1] if len(h) >= ncmp // H_EVERY else None,
+            "H_L2_fp64_at_compare": h_fp64[ncmp // H_EVERY - 1] if len(h_fp64) >= ncmp // H_EVERY else None,
             "dtype": "f32 algebra / f64 state", "H_L2": h[-1] if h else None,
             "H_L2_fp64": h_fp64[-1] if h_fp64 else None,
             "H_L2_rel_diff": (abs(h[-1] - h_fp64[-1]) / h_fp64[-1]) if h and h_fp64 else None,
@@ -580,6 +647,7 @@ def run_batched(args, world, rank, dist):
     return {"value": value, "unit": UNIT, "evolutions": len(specs), "steps": steps, "ms_per_step": ms_max / steps,
             "interior_points": pts if dist is None else None, "tile": list(tune["tile"]), "blocks": tune["blocks"],
             "autotune": tune["table"], "graph_kernel_nodes_per_replay": info["kernel_nodes"],
+            "tile_fill": info["tile_fill"],
             "sequential_single_grid_value": seq_value, "speedup_vs_sequential": value / seq_value}
 
 

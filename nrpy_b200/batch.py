@@ -19,7 +19,9 @@ import numpy as np
 
 from . import lib as L
 
-TILE_SHAPES = [(32, 4), (64, 2), (16, 8), (128, 1)]
+# (0, 0): each grid gets the 128-point brick (i0 x i1 x i2) that pads its interior least.
+PER_GRID = (0, 0)
+TILE_SHAPES = [PER_GRID, (32, 4), (64, 2), (16, 8), (128, 1)]
 
 
 def batching_workload(seed: int = 7, n: int = 64) -> List[Dict]:
@@ -72,7 +74,9 @@ class BatchedEvolutions:
     def interior_points(self) -> int:
         return sum(g.n_interior for g in self.grids)
 
-    def build(self, tile: Tuple[int, int] = (32, 4), blocks: Optional[int] = None, steps_per_graph: int = 1):
+    def build(self, tile: Tuple[int, int] = PER_GRID, blocks: Optional[int] = None, steps_per_graph: int = 1):
+        """Create the batch object and capture its graph: `tile` = (bx, by) with bx*by = 128 for
+        one shape for every grid, or PER_GRID for a brick chosen per grid."""
         import torch
 
         self.free()
@@ -94,7 +98,10 @@ class BatchedEvolutions:
         nt, no, ni = C.c_int(), C.c_int(), C.c_int()
         kn = C.c_ulonglong()
         L.check(self.lib.bssn_b200_batch_info(self._batch, C.byref(nt), C.byref(no), C.byref(ni), C.byref(kn)))
-        return {"tiles": nt.value, "outer_points": no.value, "inner_points": ni.value, "kernel_nodes": kn.value}
+        pts, padded = C.c_longlong(), C.c_longlong()
+        L.check(self.lib.bssn_b200_batch_tile_fill(self._batch, C.byref(pts), C.byref(padded)))
+        return {"tiles": nt.value, "outer_points": no.value, "inner_points": ni.value, "kernel_nodes": kn.value,
+                "tile_fill": pts.value / max(padded.value, 1)}
 
     def save_states(self):
         return [g.y_n.clone() for g in self.grids], [(g.cd.time, g.cd.nn) for g in self.grids]
@@ -162,4 +169,4 @@ def time_batch(be: BatchedEvolutions, steps: int) -> float:
     return a.elapsed_time(b)
 
 
-__all__ = ["BatchedEvolutions", "batching_workload", "partition_evolutions", "time_batch", "TILE_SHAPES"]
+__all__ = ["BatchedEvolutions", "batching_workload", "partition_evolutions", "time_batch", "TILE_SHAPES", "PER_GRID"]

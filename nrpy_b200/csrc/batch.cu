@@ -31,7 +31,8 @@ struct bssn_b200_batch {
   BatchInnerPt *d_inner = nullptr;
   int ninner = 0;
   std::vector<double *> krhs;
-  int bx = 32, by = 4, blocks = 296, steps_per_graph = 1;
+  int bx = 32, by = 4, blocks = 296, steps_per_graph = 1;  // bx = by = 0: a tile shape per evolution
+  long long padded_points = 0, interior_points = 0;          // tile capacity and interior points covered
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -41,8 +42,8 @@ struct bssn_b200_batch {
 namespace bssn {
 
 static int batch_stage(bssn_b200_batch *b, int stage, cudaStream_t s) {
-  BSSN_TRY(launch_ricci_batched(b->v, stage, b->d_descs, b->d_tile_evo, b->ntiles, b->blocks, b->bx, b->by, s));
-  BSSN_TRY(launch_rhs_fused_batched(b->v, stage, b->d_descs, b->d_tile_evo, b->ntiles, b->blocks, b->bx, b->by, s));
+  BSSN_TRY(launch_ricci_batched(b->v, stage, b->d_descs, b->d_tile_evo, b->ntiles, b->blocks, s));
+  BSSN_TRY(launch_rhs_fused_batched(b->v, stage, b->d_descs, b->d_tile_evo, b->ntiles, b->blocks, s));
   for (int gz = 0; gz < NGHOSTS; gz++)
     BSSN_TRY(launch_radiation_batched(stage, b->d_descs, b->d_outer_layer[gz], b->nouter_layer[gz], s));
   BSSN_TRY(launch_rk_points_batched(b->v, stage, b->d_descs, b->d_outer_all, b->nouter_all, s));
@@ -52,6 +53,27 @@ static int batch_stage(bssn_b200_batch *b, int stage, cudaStream_t s) {
 static int batch_step(bssn_b200_batch *b, cudaStream_t s) {
   for (int stage = 1; stage <= 4; stage++) BSSN_TRY(batch_stage(b, stage, s));
   return BSSN_B200_OK;
+}
+
+// Tile shapes (points along i0, i1, i2; 128 points) among which a batch built with per-grid
+// shapes picks, for each evolution, the one that pads its interior least (ties: the wider
+// along i0, for coalescing).
+struct Brick {
+  int bx, by, bz;
+};
+static const Brick kBricks[] = {{128, 1, 1}, {64, 2, 1}, {64, 1, 2}, {32, 4, 1}, {32, 2, 2}, {32, 1, 4},
+                                {16, 8, 1},  {16, 4, 2}, {16, 2, 4}, {16, 1, 8}};
+
+static long long padded_points(int n0, int n1, int n2, const Brick &k) {
+  return (long long)((n0 + k.bx - 1) / k.bx) * k.bx * ((n1 + k.by - 1) / k.by) * k.by * ((n2 + k.bz - 1) / k.bz) *
+         k.bz;
+}
+
+static Brick best_brick(int n0, int n1, int n2) {
+  Brick best = kBricks[0];
+  for (const Brick &k : kBricks)
+    if (padded_points(n0, n1, n2, k) < padded_points(n0, n1, n2, best)) best = k;
+  return best;
 }
 
 template <typename Tp>
@@ -118,10 +140,16 @@ static int batch_build(bssn_b200_batch *b) {
     d.AMPL = G.params.AMPL;
     d.SINHW = G.params.SINHW;
     const int n0 = d.g.N0 - 2 * NGHOSTS, n1 = d.g.N1 - 2 * NGHOSTS, n2 = d.g.N2 - 2 * NGHOSTS;
-    d.tiles_x = (n0 + b->bx - 1) / b->bx;
-    d.tiles_y = (n1 + b->by - 1) / b->by;
+    const Brick k = b->bx == 0 ? best_brick(n0, n1, n2) : Brick{b->bx, b->by, 1};
+    d.tile_bx = k.bx;
+    d.tile_by = k.by;
+    d.tile_bz = k.bz;
+    d.tiles_x = (n0 + k.bx - 1) / k.bx;
+    d.tiles_y = (n1 + k.by - 1) / k.by;
     d.tile_begin = (int)tile_evo.size();
-    const long long nt = (long long)d.tiles_x * d.tiles_y * std::max(n2, 0);
+    const long long nt = (long long)d.tiles_x * d.tiles_y * ((std::max(n2, 0) + k.bz - 1) / k.bz);
+    b->padded_points += padded_points(n0, n1, std::max(n2, 0), k);
+    b->interior_points += (long long)n0 * n1 * std::max(n2, 0);
     if ((long long)tile_evo.size() + nt > (1LL << 30)) {
       set_error("batch: too many tiles");
       return BSSN_B200_EINVAL;
@@ -177,10 +205,11 @@ int bssn_b200_batch_create(int nevo, commondata_struct *const *cds, griddata_str
     set_error("batch: need nevo >= 1 and non-NULL arrays");
     return BSSN_B200_EINVAL;
   }
-  if (tile_bx * tile_by != 128 || tile_bx < 1 || tile_by < 1 || blocks < 1 || steps_per_graph < 1 ||
+  const bool per_grid = tile_bx == 0 && tile_by == 0;
+  if ((!per_grid && (tile_bx * tile_by != 128 || tile_bx < 1 || tile_by < 1)) || blocks < 1 || steps_per_graph < 1 ||
       steps_per_graph > 1000) {
-    set_error("batch: tile %dx%d must have 128 points; blocks >= 1; 1 <= steps_per_graph <= 1000", tile_bx,
-              tile_by);
+    set_error("batch: tile %dx%d must have 128 points (or 0x0: a shape per evolution); blocks >= 1; "
+              "1 <= steps_per_graph <= 1000", tile_bx, tile_by);
     return BSSN_B200_EINVAL;
   }
   if (!stream) {
@@ -281,6 +310,16 @@ int bssn_b200_batch_run(bssn_b200_batch *b, int graph_launches) {
       }
     }
   }
+  return BSSN_B200_OK;
+}
+
+int bssn_b200_batch_tile_fill(const bssn_b200_batch *b, long long *interior_points, long long *padded_points) {
+  if (!b) {
+    set_error("batch_tile_fill: NULL batch");
+    return BSSN_B200_EINVAL;
+  }
+  if (interior_points) *interior_points = b->interior_points;
+  if (padded_points) *padded_points = b->padded_points;
   return BSSN_B200_OK;
 }
 

@@ -161,6 +161,7 @@ struct EvoDesc {
   int radial_sinh;  // 0: r = xx0 ; 1: SinhSpherical r(xx0)
   double AMPL, SINHW;
   int tile_begin, tiles_x, tiles_y;  // this evolution's tiles in the batch tile list
+  int tile_bx, tile_by, tile_bz;     // its tile shape: tile_bx * tile_by * tile_bz = 128 points
 };
 struct BatchOuterPt {
   int evo;
@@ -179,12 +180,11 @@ __host__ __device__ inline void stage_io(const EvoDesc &d, int stage, double *&k
   }
 }
 // Batched launchers (pointwise.cu, boundary.cu): one launch covers every evolution.
-// `blocks` is the persistent grid size; the block shape (bx, by) with bx*by = 128 is the
-// tile shape the tile list was built for.
+// `blocks` is the persistent grid size; each evolution's tile shape is in its EvoDesc.
 int launch_ricci_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                         int bx, int by, cudaStream_t s);
+                         cudaStream_t s);
 int launch_rhs_fused_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                             int bx, int by, cudaStream_t s);
+                             cudaStream_t s);
 int launch_radiation_batched(int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts, cudaStream_t s);
 int launch_rk_points_batched(Variant v, int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts,
                              cudaStream_t s);

@@ -211,6 +211,7 @@ SIGNATURES = [
     ("bssn_b200_batch_run", C.c_int, [V, C.c_int]),
     ("bssn_b200_batch_info", C.c_int, [V, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                        C.POINTER(C.c_ulonglong)]),
+    ("bssn_b200_batch_tile_fill", C.c_int, [V, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     ("bssn_b200_batch_destroy", C.c_int, [V]),
     ("bssn_b200_adjoint_create", C.c_int, [PCD, PGD, C.c_int, C.c_int, V, C.POINTER(V)]),
     ("bssn_b200_adjoint_forward", C.c_int, [V, C.POINTER(C.c_double)]),

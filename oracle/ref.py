@@ -252,6 +252,33 @@ class RefGrid:
                     out[i2, i1, i0] = self.lib.ref_dV(self.h, i0, i1, i2)
         return out
 
+    def interior_dV(self) -> np.ndarray:
+        """The reference's volume element sqrt(det gammahat) dxx0 dxx1 dxx2 on the interior
+        (shape (N2-2G, N1-2G, N0-2G)), from its own rfm arrays (|f0' f0^2 f1| dxx0 dxx1 dxx2,
+        Spherical family), spot-checked against its dV() at a few points."""
+        G = self.nghosts
+        N0, N1, N2 = self.N
+        f0, f0_D0, f1 = self.rfm_field(0, N0), self.rfm_field(1, N0), self.rfm_field(4, N1)
+        x0, x1, x2 = self.xx()
+        dvol = abs((x0[1] - x0[0]) * (x1[1] - x1[0]) * (x2[1] - x2[0]))
+        dV = np.abs(f0_D0[None, None, :] * f0[None, None, :] ** 2 * f1[None, :, None]) * dvol
+        dV = np.ascontiguousarray(np.broadcast_to(dV, (N2, N1, N0))[G:-G, G:-G, G:-G])
+        rng = np.random.default_rng(0)
+        for _ in range(4):
+            i0, i1, i2 = (int(rng.integers(G, n - G)) for n in (N0, N1, N2))
+            ref_dv = self.lib.ref_dV(self.h, i0, i1, i2)
+            if abs(dV[i2 - G, i1 - G, i0 - G] - ref_dv) > 1e-12 * abs(ref_dv):
+                raise RuntimeError("volume element differs from the reference's dV()")
+        return dV
+
+    def h_l2(self, y: np.ndarray, dV: np.ndarray = None) -> float:
+        """sqrt(sum over the interior of H^2 dV): the reference's Ricci_eval + constraints_eval
+        and its volume-integration measure, on state y."""
+        G = self.nghosts
+        dV = self.interior_dV() if dV is None else dV
+        H = self.constraints(y, self.ricci(y))[0].reshape(self.N[2], self.N[1], self.N[0])[G:-G, G:-G, G:-G]
+        return float(np.sqrt((H**2 * dV).sum()))
+
     def bcstruct(self):
         """(inner: structured array dstpt/srcpt/parity, outer: {(gz,dirn): array i0,i1,i2,FACEX0..2})."""
         inner_dt = np.dtype([("dstpt", "<i4"), ("srcpt", "<i4"), ("parity", "i1", (10,)), ("_pad", "V2")])

@@ -19,7 +19,7 @@ SPECS = [
 ]
 
 
-@pytest.mark.parametrize("tile", [(32, 4), (64, 2)])
+@pytest.mark.parametrize("tile", [(32, 4), (64, 2), (0, 0)])
 def test_batch_equals_single_grid_path(cuda, tile):
     from nrpy_b200.batch import BatchedEvolutions
     from nrpy_b200.grid import BSSNGrid
