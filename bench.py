@@ -284,6 +284,10 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=100)
+    ap.add_argument("--batch-tile", default=None,
+                    help="batched tile shape bx,by (0,0: a shape per grid) instead of the autotuner's pick")
+    ap.add_argument("--no-batch-sequential", action="store_true",
+                    help="skip advancing the batched grids one at a time (profiling)")
     ap.add_argument("--no-diff", action="store_true", help="skip the adjoint-gradient section")
     ap.add_argument("--no-diag", action="store_true", help="skip the diagnostics-output section")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own CUDA build")
@@ -610,7 +614,12 @@ def run_batched(args, world, rank, dist):
     sizes = [s["Nxx"][0] * s["Nxx"][1] * s["Nxx"][2] for s in specs]
     mine = partition_evolutions(sizes, world)[rank]
     be = BatchedEvolutions([specs[i] for i in mine])
-    tune = be.autotune(steps=2)
+    if args.batch_tile:
+        bx, by = (int(x) for x in args.batch_tile.split(","))
+        tune = {"tile": (bx, by), "blocks": 4 * torch.cuda.get_device_properties(be.device).multi_processor_count,
+                "table": "not run (--batch-tile)"}
+    else:
+        tune = be.autotune(steps=2)
     spg = 20
     be.build(tile=tune["tile"], blocks=tune["blocks"], steps_per_graph=spg)
     be.run(1)
@@ -629,7 +638,7 @@ def run_batched(args, world, rank, dist):
     # the same evolutions one grid at a time (single-grid CUDA graphs), a few steps each
     seq_steps = 10
     seq_ms = 0.0
-    for g in be.grids:
+    for g in ([] if args.no_batch_sequential else be.grids):
         st = g.make_stepper(mode=1, steps_per_graph=seq_steps)
         with torch.cuda.stream(st):
             g.run_stepper(1)
@@ -642,13 +651,14 @@ def run_batched(args, world, rank, dist):
         b2.synchronize()
         seq_ms += a2.elapsed_time(b2)
         g.free_stepper()
-    seq_value, _ = aggregate(pts, seq_steps, seq_ms, dist, device="cuda")
+    seq_value = aggregate(pts, seq_steps, seq_ms, dist, device="cuda")[0] if seq_ms > 0 else None
     be.close()
     return {"value": value, "unit": UNIT, "evolutions": len(specs), "steps": steps, "ms_per_step": ms_max / steps,
             "interior_points": pts if dist is None else None, "tile": list(tune["tile"]), "blocks": tune["blocks"],
             "autotune": tune["table"], "graph_kernel_nodes_per_replay": info["kernel_nodes"],
             "tile_fill": info["tile_fill"],
-            "sequential_single_grid_value": seq_value, "speedup_vs_sequential": value / seq_value}
+            "sequential_single_grid_value": seq_value,
+            "speedup_vs_sequential": value / seq_value if seq_value else None}
 
 
 def run_diagnostics(grid, args, reps: int = 3):

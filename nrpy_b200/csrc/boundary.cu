@@ -260,26 +260,31 @@ int launch_radiation_batched(int stage, const EvoDesc *descs, const BatchOuterPt
   return BSSN_B200_OK;
 }
 
-// Parity copies into every inner ghost point of every evolution's stage output.
+// Parity copies into every inner ghost point of every evolution's stage output. One thread
+// per inner point copies all 24 gridfunctions: the point's record and its evolution's
+// descriptor are read once, and a warp's 32 consecutive records (mostly consecutive dstpt
+// and srcpt along i0) make each gridfunction's loads and stores contiguous.
 __global__ void inner_batched_kernel(const EvoDesc *__restrict__ descs, const BatchInnerPt *__restrict__ pts,
                                      const int npts, const int stage) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= npts * NUM_EVOL_GFS) return;
-  const int gf = t / npts;
-  const BatchInnerPt q = pts[t - gf * npts];
+  if (t >= npts) return;
+  const BatchInnerPt q = pts[t];
   const EvoDesc &d = descs[q.evo];
   double *kin, *kout;
   stage_io(d, stage, kin, kout);
-  double *g = kout + (size_t)gf * d.g.ntot;
+  const size_t ntot = (size_t)d.g.ntot;
   constexpr int8_t parity[NUM_EVOL_GFS] = {4, 5, 6, 7, 8, 9, 0, 1, 2, 3, 0, 4, 5, 6, 7, 8, 9, 1, 2, 3, 0, 1, 2, 3};
-  g[q.b.dstpt] = flip_sign(g[q.b.srcpt], q.b.parity[parity[gf]]);
+  double v[NUM_EVOL_GFS];
+#pragma unroll
+  for (int gf = 0; gf < NUM_EVOL_GFS; gf++) v[gf] = kout[q.b.srcpt + gf * ntot];
+#pragma unroll
+  for (int gf = 0; gf < NUM_EVOL_GFS; gf++) kout[q.b.dstpt + gf * ntot] = flip_sign(v[gf], q.b.parity[parity[gf]]);
 }
 
 int launch_inner_batched(int stage, const EvoDesc *descs, const BatchInnerPt *pts, int npts, cudaStream_t s) {
   if (npts <= 0) return BSSN_B200_OK;
-  const int threads = 256;
-  const long long work = (long long)npts * NUM_EVOL_GFS;
-  inner_batched_kernel<<<(unsigned)((work + threads - 1) / threads), threads, 0, s>>>(descs, pts, npts, stage);
+  const int threads = 128;
+  inner_batched_kernel<<<(unsigned)((npts + threads - 1) / threads), threads, 0, s>>>(descs, pts, npts, stage);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }

@@ -6,15 +6,22 @@ nrpy/examples/two_blackholes_collide.py:60-440 with the settings the workloads n
 
 * Kreiss-Oliger dissipation ON (the example has it off, two_blackholes_collide.py:124),
   CAKO on, strengths 0.3 (rhs_eval.py:48-49);
-* CoordSystem Spherical or SinhSpherical; ``--axisym`` sets symmetry_axes="2"
-  (two_blackholes_collide.py:141-143), otherwise the grid is full 3-D;
+* CoordSystem Spherical, SinhSpherical or SinhCylindrical; ``--axisym`` sets the
+  axisymmetry axis of the coordinate system (symmetry_axes="2", the phi index of the
+  Spherical family, two_blackholes_collide.py:141-143; "1" for the cylindrical family,
+  blackhole_spectroscopy.py:153), otherwise the grid is full 3-D;
+* SinhCylindrical as blackhole_spectroscopy.py:60-160 sets it up: AMPLRHO = AMPLZ =
+  grid_physical_size, SINHWRHO = SINHWZ = 0.2, CFL_FACTOR 0.5;
 * the BHaHAHA horizon finder off (it is a diagnostic, not the step);
 * every coordinate system's CodeParameters registered ("All"), so that one
   params_struct layout serves every project variant;
 * ``--checkpoint`` also registers write_checkpoint/read_checkpoint (checkpointing.py:473-490),
   which adds the REAL CodeParameter checkpoint_every to commondata_struct;
 * ``--fd-order N`` sets the interior finite-difference order (4 by default; NGHOSTS = N/2 + 1),
-  the outer radiation condition staying at radiation_BC_fd_order = 4.
+  the outer radiation condition staying at radiation_BC_fd_order = 4;
+* the reference metrics of Spherical, SinhSpherical and SinhCylindrical are all instantiated,
+  so that every variant's params_struct carries the CodeParameters of all three and one
+  layout serves every project variant.
 
 Run it with the reference on PYTHONPATH (oracle/gen_ref.py does this).
 """
@@ -46,10 +53,10 @@ par.set_parval_from_str("fp_type", "double")
 CoordSystem = args.coord
 set_of_CoordSystems = {CoordSystem}
 grid_physical_size = 7.5 if CoordSystem == "Spherical" else 10.0
-Nxx_dict = {"Spherical": [72, 12, 2], "SinhSpherical": [256, 64, 64]}
+Nxx_dict = {"Spherical": [72, 12, 2], "SinhSpherical": [256, 64, 64], "SinhCylindrical": [128, 2, 256]}
 OMP_collapse = 2
 if args.axisym:
-    par.set_parval_from_str("symmetry_axes", "2")
+    par.set_parval_from_str("symmetry_axes", "1" if "Cylindrical" in CoordSystem else "2")
 
 project_dir = args.project_dir
 shutil.rmtree(project_dir, ignore_errors=True)
@@ -59,7 +66,7 @@ par.set_parval_from_str("CoordSystem_to_register_CodeParameters", "All")
 # Instantiate both reference metrics so that both register their CodeParameters
 # (RMAX for Spherical; AMPL, SINHW for SinhSpherical): every variant then shares one
 # params_struct layout.
-for _coord in ("Spherical", "SinhSpherical"):
+for _coord in ("Spherical", "SinhSpherical", "SinhCylindrical"):
     _ = refmetric.reference_metric[_coord]
 
 if parallelization == "cuda":
@@ -179,6 +186,12 @@ BHaH.rfm_wrapper_functions.register_CFunctions_CoordSystem_wrapper_funcs()
 par.adjust_CodeParam_default("t_final", grid_physical_size)
 if CoordSystem == "SinhSpherical":
     par.adjust_CodeParam_default("SINHW", 0.2)
+if CoordSystem == "SinhCylindrical":
+    par.adjust_CodeParam_default("AMPLRHO", grid_physical_size)
+    par.adjust_CodeParam_default("AMPLZ", grid_physical_size)
+    par.adjust_CodeParam_default("SINHWRHO", 0.2)
+    par.adjust_CodeParam_default("SINHWZ", 0.2)
+    par.adjust_CodeParam_default("CFL_FACTOR", 0.5)
 par.adjust_CodeParam_default("eta", 1.0)
 par.adjust_CodeParam_default("BH1_mass", 0.5)
 par.adjust_CodeParam_default("BH2_mass", 0.5)
