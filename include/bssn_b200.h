@@ -70,6 +70,7 @@ enum {
 /* CoordSystem_hash values (BHaH_defines.h). */
 #define SPHERICAL 1307621703
 #define SINHSPHERICAL 579707936
+#define SINHCYLINDRICAL 1325205359
 
 /* commondata_struct: CodeParameters shared by all grids (BHaH_defines_h.py, CodeParameters.py:17-199). */
 typedef struct __commondata_struct__ {
@@ -102,12 +103,19 @@ typedef struct __commondata_struct__ {
 /* params_struct: per-grid CodeParameters (BHaH_defines_h.py; numerical_grids_and_timestep.py). */
 typedef struct __params_struct__ {
   REAL AMPL;
+  REAL AMPLRHO;
+  REAL AMPLZ;
   REAL Cart_originx;
   REAL Cart_originy;
   REAL Cart_originz;
   REAL PI;
+  REAL RHOMAX;
   REAL RMAX;
   REAL SINHW;
+  REAL SINHWRHO;
+  REAL SINHWZ;
+  REAL ZMAX;
+  REAL ZMIN;
   REAL dxx0;
   REAL dxx1;
   REAL dxx2;
@@ -143,8 +151,11 @@ typedef struct __params_struct__ {
 } params_struct;
 
 /* rfm_struct: 1-D reference-metric precompute arrays (rfm_precompute.py:84-565). The
- * SinhSpherical field list is used for both coordinate systems; for Spherical the radial
- * derivatives are 1, 0, 0. Array members are device pointers. */
+ * SinhSpherical field list is used for the Spherical family (for Spherical the radial
+ * derivatives are 1, 0, 0). A SinhCylindrical project's rfm_struct has the same seven
+ * pointers with f3_of_xx2, f3_of_xx2__D2, f3_of_xx2__DD22 (functions of xx2, arrays of
+ * Nxx_plus_2NGHOSTS2 entries) in the last three places, which the library reads through
+ * these names. Array members are device pointers. */
 typedef struct __rfmstruct__ {
   REAL *f0_of_xx0;
   REAL *f0_of_xx0__D0;

@@ -41,6 +41,12 @@ RFM_FIELDS = {
     "f1_of_xx1": ("rfm_f1", 1),
     "f1_of_xx1__D1": ("rfm_f1_D1", 1),
     "f1_of_xx1__DD11": ("rfm_f1_DD11", 1),
+    # Cylindrical family: the second function of the reference metric depends on xx2 and
+    # takes the same three rfm_struct slots (SinhCylindrical's rfm_struct lists f3_of_xx2*
+    # where the Spherical family lists f1_of_xx1*).
+    "f3_of_xx2": ("rfm_f1", 2),
+    "f3_of_xx2__D2": ("rfm_f1_D1", 2),
+    "f3_of_xx2__DD22": ("rfm_f1_DD11", 2),
 }
 SCALAR_PARAMS = {"eta", "KreissOliger_strength_gauge", "KreissOliger_strength_nongauge"}
 

@@ -23,6 +23,8 @@ VARIANTS = {
     "sph_3d": ("Spherical", ""),
     "sinh_axi": ("SinhSpherical", "2"),
     "sinh_3d": ("SinhSpherical", ""),
+    # SinhCylindrical with symmetry_axes="1" (axisymmetry about z), as blackhole_spectroscopy.py sets it up
+    "sinhcyl_axi": ("SinhCylindrical", "1"),
 }
 
 

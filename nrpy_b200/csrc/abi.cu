@@ -33,9 +33,16 @@ int variant_of(const params_struct *p, Variant *out) {
   const bool axi = (g_sym_mask & 4) != 0;
   if (p->CoordSystem_hash == SPHERICAL) *out = axi ? SPH_AXI : SPH_3D;
   else if (p->CoordSystem_hash == SINHSPHERICAL) *out = axi ? SINH_AXI : SINH_3D;
-  else {
-    set_error("CoordSystem_hash %d not supported (Spherical=%d, SinhSpherical=%d)", p->CoordSystem_hash, SPHERICAL,
-              SINHSPHERICAL);
+  else if (p->CoordSystem_hash == SINHCYLINDRICAL) {
+    // SinhCylindrical is built axisymmetric about z (symmetry_axes "1"), as blackhole_spectroscopy runs it.
+    if (g_sym_mask != 2) {
+      set_error("SinhCylindrical is built with symmetry_axes \"1\" only (set it before the set-up)");
+      return BSSN_B200_EINVAL;
+    }
+    *out = SINHCYL_AXI;
+  } else {
+    set_error("CoordSystem_hash %d not supported (Spherical=%d, SinhSpherical=%d, SinhCylindrical=%d)",
+              p->CoordSystem_hash, SPHERICAL, SINHSPHERICAL, SINHCYLINDRICAL);
     return BSSN_B200_EINVAL;
   }
   return BSSN_B200_OK;
@@ -136,8 +143,9 @@ int bssn_b200_set_symmetry_axes(const char *axes) {
       mask |= 1 << (*c - '0');
     }
   }
-  if (mask != 0 && mask != 4) {
-    set_error("symmetry axes \"%s\": only \"\" (3-D) and \"2\" (axisymmetric) are generated", axes ? axes : "");
+  if (mask != 0 && mask != 4 && mask != 2) {
+    set_error("symmetry axes \"%s\": only \"\" (3-D), \"2\" (axisymmetric Spherical family) and \"1\" "
+              "(axisymmetric SinhCylindrical) are generated", axes ? axes : "");
     return BSSN_B200_EINVAL;
   }
   g_sym_mask = mask;

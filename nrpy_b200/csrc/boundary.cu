@@ -129,6 +129,61 @@ __global__ void radiation_kernel(const GridDims g, const RadialMap rm, const dou
   rhs[idx + (size_t)gf * g.ntot] = out_here + k * rinv * rinv * rinv;
 }
 
+// The same 4th-order first derivative along a direction of index stride `st` (i2: s2).
+__device__ __forceinline__ double fd1_dir(const double *__restrict__ f, int idx, int st, int offset, double invdx) {
+  switch (offset) {
+    case 0:
+      return ((1.0 / 12.0) * f[idx - 2 * st] - (2.0 / 3.0) * f[idx - st] + (2.0 / 3.0) * f[idx + st] -
+              (1.0 / 12.0) * f[idx + 2 * st]) * invdx;
+    case 1:
+      return (-(1.0 / 4.0) * f[idx - st] - (5.0 / 6.0) * f[idx] + (3.0 / 2.0) * f[idx + st] -
+              (1.0 / 2.0) * f[idx + 2 * st] + (1.0 / 12.0) * f[idx + 3 * st]) * invdx;
+    case -1:
+      return (-(1.0 / 12.0) * f[idx - 3 * st] + (1.0 / 2.0) * f[idx - 2 * st] - (3.0 / 2.0) * f[idx - st] +
+              (5.0 / 6.0) * f[idx] + (1.0 / 4.0) * f[idx + st]) * invdx;
+    case 2:
+      return (-(25.0 / 12.0) * f[idx] + 4.0 * f[idx + st] - 3.0 * f[idx + 2 * st] + (4.0 / 3.0) * f[idx + 3 * st] -
+              (1.0 / 4.0) * f[idx + 4 * st]) * invdx;
+    default:  // -2
+      return ((1.0 / 4.0) * f[idx - 4 * st] - (4.0 / 3.0) * f[idx - 3 * st] + 3.0 * f[idx - 2 * st] -
+              4.0 * f[idx - st] + (25.0 / 12.0) * f[idx]) * invdx;
+  }
+}
+
+// SinhCylindrical: r = sqrt(rho^2 + z^2) has partial derivatives along xx0 and xx2, so
+// partial_r f = (dx0/dr) d_x0 f + (dx2/dr) d_x2 f, each one-sided FD shifted away from the
+// face and from the grid's edges as in the reference's compute_partial_r_f.
+__global__ void radiation_cyl_kernel(const GridDims g, const CylMap cm, const double *__restrict__ xx0,
+                                     const double *__restrict__ xx2, const outerpt_bc_struct *__restrict__ pts,
+                                     const int npts, const double *__restrict__ gfs, double *__restrict__ rhs,
+                                     const GfTable tab) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= npts * NUM_EVOL_GFS) return;
+  const int gf = t / npts;
+  const int pt = t - gf * npts;
+  const outerpt_bc_struct p = pts[pt];
+  const int i0 = p.i0, i1 = p.i1, i2 = p.i2;
+  const int j0 = i0 + p.FACEX0, j1 = i1 + p.FACEX1, j2 = i2 + p.FACEX2;
+  double r, dx0dr, dx2dr, r_int, dx0dr_int, dx2dr_int;
+  cm.radial(xx0[i0], xx2[i2], r, dx0dr, dx2dr);
+  cm.radial(xx0[j0], xx2[j2], r_int, dx0dr_int, dx2dr_int);
+  const double *f = gfs + (size_t)gf * g.ntot;
+  const int idx = i0 + g.s1 * i1 + g.s2 * i2;
+  const int idx_int = j0 + g.s1 * j1 + g.s2 * j2;
+  const double dfdr = dx0dr * fd1_dir(f, idx, 1, fd1_offset(i0, p.FACEX0, g.N0), g.invdxx0) +
+                      dx2dr * fd1_dir(f, idx, g.s2, fd1_offset(i2, p.FACEX2, g.N2), g.invdxx2);
+  const double dfdr_int = dx0dr_int * fd1_dir(f, idx_int, 1, fd1_offset(j0, p.FACEX0, g.N0), g.invdxx0) +
+                          dx2dr_int * fd1_dir(f, idx_int, g.s2, fd1_offset(j2, p.FACEX2, g.N2), g.invdxx2);
+  const double c = tab.wavespeed[gf], finf = tab.finf[gf];
+  const double dtf_int = rhs[idx_int + (size_t)gf * g.ntot];
+  const double fv = f[idx], fv_int = f[idx_int];
+  const double out_int = -c * (dfdr_int + (fv_int - finf) / r_int);
+  const double k = r_int * r_int * r_int * (dtf_int - out_int);
+  const double rinv = 1.0 / r;
+  const double out_here = -c * (dfdr + (fv - finf) * rinv);
+  rhs[idx + (size_t)gf * g.ntot] = out_here + k * rinv * rinv * rinv;
+}
+
 int radial_map(const params_struct *p, RadialMap *rm) {
   if (p->CoordSystem_hash == SPHERICAL) {
     *rm = RadialMap{0, 0.0, 0.0};
@@ -144,13 +199,28 @@ int radial_map(const params_struct *p, RadialMap *rm) {
 int launch_radiation_bcs(const GridDims &g, const params_struct *p, const bc_struct *bc, const double *const xx[3],
                          const double *wavespeed, const double *f_inf, const double *gfs, double *rhs,
                          cudaStream_t s) {
-  RadialMap rm;
-  BSSN_TRY(radial_map(p, &rm));
   GfTable tab{};
   for (int k = 0; k < NUM_EVOL_GFS; k++) {
     tab.wavespeed[k] = wavespeed ? wavespeed[k] : kWavespeed[k];
     tab.finf[k] = f_inf ? f_inf[k] : kFInfinity[k];
   }
+  if (p->CoordSystem_hash == SINHCYLINDRICAL) {
+    // layer by layer and face direction by face direction, as the reference orders them
+    const CylMap cm = cyl_map(p);
+    for (int gz = 0; gz < NGHOSTS; gz++)
+      for (int dirn = 0; dirn < 3; dirn++) {
+        const int n = bc->bc_info.num_pure_outer_boundary_points[gz][dirn];
+        if (n <= 0) continue;
+        const int threads = 256;
+        const long long work = (long long)n * NUM_EVOL_GFS;
+        radiation_cyl_kernel<<<(unsigned)((work + threads - 1) / threads), threads, 0, s>>>(
+            g, cm, xx[0], xx[2], bc->pure_outer_bc_array[dirn + 3 * gz], n, gfs, rhs, tab);
+        BSSN_LAUNCH_CHECK();
+      }
+    return BSSN_B200_OK;
+  }
+  RadialMap rm;
+  BSSN_TRY(radial_map(p, &rm));
   for (int gz = 0; gz < NGHOSTS; gz++) {
     for (int dirn = 0; dirn < 3; dirn++) {
       const int n = bc->bc_info.num_pure_outer_boundary_points[gz][dirn];

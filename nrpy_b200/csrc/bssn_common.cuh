@@ -44,7 +44,7 @@ void count_launch(unsigned long long n);
 
 // ---------------------------------------------------------------- variants
 // Generated algebra variants: CoordSystem x symmetry axes.
-enum Variant { SPH_3D = 0, SPH_AXI = 1, SINH_3D = 2, SINH_AXI = 3, NUM_VARIANTS = 4 };
+enum Variant { SPH_3D = 0, SPH_AXI = 1, SINH_3D = 2, SINH_AXI = 3, SINHCYL_AXI = 4, NUM_VARIANTS = 5 };
 int symmetry_axes_mask();  // bit d set: derivatives in direction d vanish
 int variant_of(const params_struct *params, Variant *out);
 
@@ -133,6 +133,33 @@ struct RadialMap {
 };
 
 int radial_map(const params_struct *p, RadialMap *rm);
+
+// SinhCylindrical (reference_metric.py:1593-1630): rho = AMPLRHO sinh(xx0/SINHWRHO)/sinh(1/SINHWRHO),
+// phi = xx1, z = AMPLZ sinh(xx2/SINHWZ)/sinh(1/SINHWZ), in the expression trees of the
+// generated rfm_precompute_defines.
+struct CylMap {
+  double AMPLRHO, SINHWRHO, AMPLZ, SINHWZ;
+  __host__ __device__ static double sinhv(double x, double A, double w) {
+    return A * (exp(x / w) - exp(-x / w)) / (exp((1.0 / (w))) - exp(-1 / w));
+  }
+  __host__ __device__ static double dsinhv(double x, double A, double w) {
+    return A * (exp(x / w) / w + exp(-x / w) / w) / (exp((1.0 / (w))) - exp(-1 / w));
+  }
+  __host__ __device__ double rho(double xx0) const { return sinhv(xx0, AMPLRHO, SINHWRHO); }
+  __host__ __device__ double drho(double xx0) const { return dsinhv(xx0, AMPLRHO, SINHWRHO); }
+  __host__ __device__ double z(double xx2) const { return sinhv(xx2, AMPLZ, SINHWZ); }
+  __host__ __device__ double dz(double xx2) const { return dsinhv(xx2, AMPLZ, SINHWZ); }
+  // r = sqrt(rho^2 + z^2) and partial x^i / partial r at fixed spherical angles (the
+  // reference's r_and_partial_xi_partial_r_derivs, apply_bcs_outerradiation_and_inner.py:46-120):
+  // dx0/dr = (rho/r)/rho'(xx0), dx1/dr = 0, dx2/dr = (z/r)/z'(xx2).
+  __host__ __device__ void radial(double xx0, double xx2, double &r, double &dx0dr, double &dx2dr) const {
+    const double rh = rho(xx0), zz = z(xx2);
+    r = sqrt(rh * rh + zz * zz);
+    dx0dr = rh / (r * drho(xx0));
+    dx2dr = zz / (r * dz(xx2));
+  }
+};
+inline CylMap cyl_map(const params_struct *p) { return CylMap{p->AMPLRHO, p->SINHWRHO, p->AMPLZ, p->SINHWZ}; }
 
 // Boundary conditions implemented in boundary.cu.
 int launch_inner_bcs(const GridDims &g, const bc_struct *bc, double *gfs, int num_gfs, const int8_t *parity_types,

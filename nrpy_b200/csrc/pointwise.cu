@@ -27,7 +27,7 @@ struct PointCtx {
   const double *__restrict__ in;   // in_gfs + IDX3(i0,i1,i2)
   const double *__restrict__ aux;  // auxevol_gfs + IDX3(i0,i1,i2)
   int s1, s2, ntot;
-  int i0, i1;
+  int i0, i1, i2;
   double invdxx0, invdxx1, invdxx2;
   RfmArrays rfm;
   double eta, KreissOliger_strength_gauge, KreissOliger_strength_nongauge;
@@ -40,7 +40,7 @@ struct PointCtx {
 // Point values held in registers (pointwise operators without stencils).
 struct RegCtx {
   const double *v;  // NUM_EVOL_GFS values of this point
-  int i0, i1;
+  int i0, i1, i2;
   RfmArrays rfm;
   __device__ __forceinline__ double ld(int gf, int, int, int) const { return v[gf]; }
 };
@@ -67,11 +67,13 @@ struct RegCtx {
 #include "gen/bssn_sinh_axi.cuh"
 #include "gen/bssn_sph_3d.cuh"
 #include "gen/bssn_sph_axi.cuh"
+#include "gen/bssn_sinhcyl_axi.cuh"
 #elif BSSN_B200_FD_ORDER == 8
 #include "gen/bssn_sinh_3d_fd8.cuh"
 #include "gen/bssn_sinh_axi_fd8.cuh"
 #include "gen/bssn_sph_3d_fd8.cuh"
 #include "gen/bssn_sph_axi_fd8.cuh"
+#include "gen/bssn_sinhcyl_axi_fd8.cuh"
 #else
 #error "BSSN_B200_FD_ORDER: generated algebra exists for 4 and 8"
 #endif
@@ -85,17 +87,22 @@ struct RegCtx {
 template <Variant V, int G>
 using RicciG = std::conditional_t<
     V == SPH_3D, RicciGroup_sph_3d<G>,
-    std::conditional_t<V == SPH_AXI, RicciGroup_sph_axi<G>,
-                       std::conditional_t<V == SINH_3D, RicciGroup_sinh_3d<G>, RicciGroup_sinh_axi<G>>>>;
+    std::conditional_t<
+        V == SPH_AXI, RicciGroup_sph_axi<G>,
+        std::conditional_t<V == SINH_3D, RicciGroup_sinh_3d<G>,
+                           std::conditional_t<V == SINH_AXI, RicciGroup_sinh_axi<G>, RicciGroup_sinhcyl_axi<G>>>>>;
 template <Variant V, int G>
 using RhsG = std::conditional_t<
     V == SPH_3D, RhsGroup_sph_3d<G>,
-    std::conditional_t<V == SPH_AXI, RhsGroup_sph_axi<G>,
-                       std::conditional_t<V == SINH_3D, RhsGroup_sinh_3d<G>, RhsGroup_sinh_axi<G>>>>;
+    std::conditional_t<
+        V == SPH_AXI, RhsGroup_sph_axi<G>,
+        std::conditional_t<V == SINH_3D, RhsGroup_sinh_3d<G>,
+                           std::conditional_t<V == SINH_AXI, RhsGroup_sinh_axi<G>, RhsGroup_sinhcyl_axi<G>>>>>;
 constexpr int kRicciGroups = ricci_group_count_sph_3d, kRhsGroups = rhs_group_count_sph_3d;
 static_assert(ricci_group_count_sph_axi == kRicciGroups && ricci_group_count_sinh_3d == kRicciGroups &&
-                  ricci_group_count_sinh_axi == kRicciGroups && rhs_group_count_sph_axi == kRhsGroups &&
-                  rhs_group_count_sinh_3d == kRhsGroups && rhs_group_count_sinh_axi == kRhsGroups,
+                  ricci_group_count_sinh_axi == kRicciGroups && ricci_group_count_sinhcyl_axi == kRicciGroups &&
+                  rhs_group_count_sph_axi == kRhsGroups && rhs_group_count_sinh_3d == kRhsGroups &&
+                  rhs_group_count_sinh_axi == kRhsGroups && rhs_group_count_sinhcyl_axi == kRhsGroups,
               "every variant has the same output groups");
 
 // Calls f(std::integral_constant<int, G>) for G = G0 .. NG-1, stopping at the first error.
@@ -116,7 +123,8 @@ static int for_each_group(F &&f) {
     if constexpr (V == SPH_3D) NAME##_sph_3d<T, TF>(CTX, OUT, NOSLOTS(T));        \
     else if constexpr (V == SPH_AXI) NAME##_sph_axi<T, TF>(CTX, OUT, NOSLOTS(T)); \
     else if constexpr (V == SINH_3D) NAME##_sinh_3d<T, TF>(CTX, OUT, NOSLOTS(T)); \
-    else NAME##_sinh_axi<T, TF>(CTX, OUT, NOSLOTS(T));                            \
+    else if constexpr (V == SINH_AXI) NAME##_sinh_axi<T, TF>(CTX, OUT, NOSLOTS(T)); \
+    else NAME##_sinhcyl_axi<T, TF>(CTX, OUT, NOSLOTS(T));                         \
   } while (0)
 
 __device__ __forceinline__ PointCtx make_ctx(const GridDims &g, const RfmArrays &rfm, const double *in,
@@ -130,6 +138,7 @@ __device__ __forceinline__ PointCtx make_ctx(const GridDims &g, const RfmArrays 
   c.ntot = g.ntot;
   c.i0 = i0;
   c.i1 = i1;
+  c.i2 = i2;
   c.invdxx0 = g.invdxx0;
   c.invdxx1 = g.invdxx1;
   c.invdxx2 = g.invdxx2;
@@ -284,7 +293,8 @@ __device__ __forceinline__ void rk_update(const double k, const double y, double
 
 template <Variant V, int STAGE>
 __device__ __forceinline__ void rk_and_project_point(const GridDims &g, const RfmArrays &rfm, const StageBuffers &b,
-                                                     const int idx, const int i0, const int i1, const double *kk,
+                                                     const int idx, const int i0, const int i1, const int i2,
+                                                     const double *kk,
                                                      const double dt) {
   double o[NUM_EVOL_GFS];
 #pragma unroll
@@ -294,7 +304,7 @@ __device__ __forceinline__ void rk_and_project_point(const GridDims &g, const Rf
     rk_update<STAGE>(kk[k], b.y[a], run, o[k], dt);
     if (STAGE != 4) b.run[a] = run;
   }
-  RegCtx rc{o, i0, i1, rfm};
+  RegCtx rc{o, i0, i1, i2, rfm};
   double h[6];
   DISPATCH_POINT(enforce_point, V, double, double, rc, h);
 #pragma unroll
@@ -337,7 +347,7 @@ __device__ __forceinline__ void fused_body(const GridDims &g, const RfmArrays &r
     if (STAGE != 4) b.run[a] = run;
   }
   if constexpr (has_h) {
-    RegCtx rc{o, i0, i1, rfm};
+    RegCtx rc{o, i0, i1, i2, rfm};
     double h[6];
     DISPATCH_POINT(enforce_point, V, double, double, rc, h);
 #pragma unroll
@@ -372,7 +382,7 @@ __global__ void rk_points_kernel(const GridDims g, const RfmArrays rfm, const St
   double kk[NUM_EVOL_GFS];
 #pragma unroll
   for (int k = 0; k < NUM_EVOL_GFS; k++) kk[k] = krhs[idx + (size_t)k * g.ntot];
-  rk_and_project_point<V, STAGE>(g, rfm, b, idx, p.i0, p.i1, kk, dt);
+  rk_and_project_point<V, STAGE>(g, rfm, b, idx, p.i0, p.i1, p.i2, kk, dt);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -382,6 +392,7 @@ __global__ void rk_points_kernel(const GridDims g, const RfmArrays rfm, const St
     case SPH_AXI: { constexpr Variant VV = SPH_AXI; CALL; } break; \
     case SINH_3D: { constexpr Variant VV = SINH_3D; CALL; } break; \
     case SINH_AXI: { constexpr Variant VV = SINH_AXI; CALL; } break; \
+    case SINHCYL_AXI: { constexpr Variant VV = SINHCYL_AXI; CALL; } break; \
     default: set_error("unknown algebra variant %d", (int)v); return BSSN_B200_EINVAL; \
   }
 
@@ -620,7 +631,7 @@ __global__ void rk_points_batched_kernel(const EvoDesc *__restrict__ descs, cons
   double kk[NUM_EVOL_GFS];
 #pragma unroll
   for (int k = 0; k < NUM_EVOL_GFS; k++) kk[k] = d.krhs[idx + (size_t)k * d.g.ntot];
-  rk_and_project_point<V, STAGE>(d.g, d.rfm, b, idx, q.p.i0, q.p.i1, kk, d.dt);
+  rk_and_project_point<V, STAGE>(d.g, d.rfm, b, idx, q.p.i0, q.p.i1, q.p.i2, kk, d.dt);
 }
 
 template <Variant V, int G>

@@ -1,9 +1,8 @@
 // Volume integrals of the constraint diagnostics over the grid interior, FP64, deterministic.
 //
 // Reference: diagnostics_volume_integration_helpers.h:400-470 -- sum over interior points of
-// f^2 dV with dV = sqrt(det gammahat) |dxx0 dxx1 dxx2|. For the Spherical family
-// sqrt(det gammahat) = |f0' f0^2 f1| (f0 = r(xx0), f1 = sin(xx1)), evaluated from the rfm
-// precompute arrays. Each block reduces a fixed slice of the interior with warp shuffles
+// f^2 dV with dV = sqrt(det gammahat) |dxx0 dxx1 dxx2|, evaluated from the rfm precompute
+// arrays (volume_element). Each block reduces a fixed slice of the interior with warp shuffles
 // into a partial; a single block then adds the partials in a fixed order, so the result
 // does not depend on scheduling.
 #include <mutex>
@@ -16,6 +15,16 @@ constexpr int kRedThreads = 256;
 constexpr int kRedBlocks = 296;  // 2 x 148 SMs
 constexpr int kRedVals = 4;      // H^2 dV, (M^2)^2 dV, |Lambda|^2 dV, dV
 
+// sqrt(det gammahat) |dxx0 dxx1 dxx2| at an interior point: |f0' f0^2 f1| for the Spherical
+// family (f0 = r, f1 = sin(xx1)); |rho' rho z'| for SinhCylindrical (f0 = rho; the second
+// rfm function holds z'(xx2)).
+__device__ __forceinline__ double volume_element(const RfmArrays &rfm, const int cyl, const int i0, const int i1,
+                                                 const int i2, const double dvol) {
+  const double f0 = rfm.f0[i0];
+  if (cyl) return fabs(rfm.f0_D0[i0] * f0 * rfm.f1[i2]) * dvol;
+  return fabs(rfm.f0_D0[i0] * f0 * f0 * rfm.f1[i1]) * dvol;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -23,7 +32,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 __global__ void __launch_bounds__(kRedThreads) constraint_partials_kernel(const GridDims g, const RfmArrays rfm,
-                                                                          const double dvol,
+                                                                          const int cyl, const double dvol,
                                                                           const double *__restrict__ diag,
                                                                           double *__restrict__ partials) {
   const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
@@ -35,8 +44,7 @@ __global__ void __launch_bounds__(kRedThreads) constraint_partials_kernel(const 
     const int i1 = NGHOSTS + (int)(q % n1);
     const int i2 = NGHOSTS + (int)(q / n1);
     const int idx = i0 + g.s1 * i1 + g.s2 * i2;
-    const double f0 = rfm.f0[i0];
-    const double dV = fabs(rfm.f0_D0[i0] * f0 * f0 * rfm.f1[i1]) * dvol;
+    const double dV = volume_element(rfm, cyl, i0, i1, i2, dvol);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const double f = diag[idx + (size_t)k * g.ntot];
@@ -79,7 +87,8 @@ int constraint_integrals(const params_struct *p, const RfmArrays &rfm, const dou
     return BSSN_B200_OK;
   }
   const double dvol = fabs(p->dxx0 * p->dxx1 * p->dxx2);
-  constraint_partials_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, rfm, dvol, diag, scratch);
+  const int cyl = p->CoordSystem_hash == SINHCYLINDRICAL;
+  constraint_partials_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(g, rfm, cyl, dvol, diag, scratch);
   BSSN_LAUNCH_CHECK();
   double *res = scratch + kRedBlocks * kRedVals;
   sum_partials_kernel<<<1, 32 * kRedVals, 0, s>>>(scratch, kRedBlocks, res);
@@ -111,7 +120,7 @@ static __device__ __align__(256) double g_noalloc_scratch[(size_t)kNoAllocMaxBlo
 // order and writes its own partial; nothing accumulates across blocks or calls, so no entry
 // has to start at zero.
 __global__ void __launch_bounds__(kNoAllocThreads) constraint_partials_blocked_kernel(
-    const GridDims g, const RfmArrays rfm, const double dvol, const double *__restrict__ diag,
+    const GridDims g, const RfmArrays rfm, const int cyl, const double dvol, const double *__restrict__ diag,
     double *__restrict__ partials) {
   const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
   const long long n = (long long)n0 * n1 * n2;
@@ -125,8 +134,7 @@ __global__ void __launch_bounds__(kNoAllocThreads) constraint_partials_blocked_k
     const int i1 = NGHOSTS + (int)(q % n1);
     const int i2 = NGHOSTS + (int)(q / n1);
     const int idx = i0 + g.s1 * i1 + g.s2 * i2;
-    const double f0 = rfm.f0[i0];
-    const double dV = fabs(rfm.f0_D0[i0] * f0 * f0 * rfm.f1[i1]) * dvol;
+    const double dV = volume_element(rfm, cyl, i0, i1, i2, dvol);
 #pragma unroll
     for (int k = 0; k < 3; k++) {
       const double f = diag[idx + (size_t)k * g.ntot];
@@ -198,7 +206,8 @@ int constraint_integrals_noalloc(const params_struct *p, const RfmArrays &rfm, c
   if (rc != BSSN_B200_OK) return rc;
   const int nblocks = (int)((n + kNoAllocPtsPerBlock - 1) / kNoAllocPtsPerBlock);
   const double dvol = fabs(p->dxx0 * p->dxx1 * p->dxx2);
-  constraint_partials_blocked_kernel<<<nblocks, kNoAllocThreads, 0, s>>>(g, rfm, dvol, diag, scratch);
+  const int cyl = p->CoordSystem_hash == SINHCYLINDRICAL;
+  constraint_partials_blocked_kernel<<<nblocks, kNoAllocThreads, 0, s>>>(g, rfm, cyl, dvol, diag, scratch);
   BSSN_LAUNCH_CHECK();
   double *res = scratch + (size_t)kNoAllocMaxBlocks * kRedVals;
   sum_partials_kernel<<<1, 32 * kRedVals, 0, s>>>(scratch, nblocks, res);

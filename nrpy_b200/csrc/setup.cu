@@ -41,11 +41,18 @@ void commondata_defaults(commondata_struct *cd) {
 void params_defaults(params_struct *p) {
   memset(p, 0, sizeof(*p));
   p->AMPL = 10.0;
+  p->AMPLRHO = 10.0;
+  p->AMPLZ = 10.0;
   p->Cart_originx = p->Cart_originy = p->Cart_originz = 0.0;
   p->Nxx0 = p->Nxx1 = p->Nxx2 = 64;
   p->PI = kPI;
+  p->RHOMAX = 10.0;
   p->RMAX = 10.0;
   p->SINHW = 0.2;
+  p->SINHWRHO = 0.2;
+  p->SINHWZ = 0.2;
+  p->ZMAX = 10.0;
+  p->ZMIN = -10.0;
   p->grid_hole_radius = 2.0;
   p->grid_idx = 0;
   p->grid_physical_size = 10.0;
@@ -62,21 +69,35 @@ void params_defaults(params_struct *p) {
 }
 
 // ---------------------------------------------------------------- coordinates
-// xx -> Cartesian for the Spherical family, r(xx0) from reference_metric.py:1195-1330.
+// xx -> Cartesian. Spherical family: r(xx0) from reference_metric.py:1195-1330;
+// SinhCylindrical: rho(xx0), phi = xx1, z(xx2) from reference_metric.py:1593-1630.
+enum CoordKind { COORD_SPHERICAL = 0, COORD_SINHSPHERICAL = 1, COORD_SINHCYLINDRICAL = 2 };
 struct Coord {
-  int sinh;
-  double AMPL, SINHW;
+  int kind;
+  double AMPL, SINHW;  // SinhSpherical
+  CylMap cyl;          // SinhCylindrical
+  __host__ __device__ bool cylindrical() const { return kind == COORD_SINHCYLINDRICAL; }
   __host__ __device__ double r(double xx0) const {
-    if (!sinh) return xx0;
+    if (kind == COORD_SPHERICAL) return xx0;
     const double tmp0 = 1.0 / SINHW;
     return AMPL * (exp(tmp0 * xx0) - exp(-tmp0 * xx0)) / (exp(tmp0) - exp(-tmp0));
   }
   __host__ __device__ double drdx0(double xx0) const {
-    if (!sinh) return 1.0;
+    if (kind == COORD_SPHERICAL) return 1.0;
     const double tmp0 = 1.0 / SINHW;
     return AMPL * (exp(tmp0 * xx0) * tmp0 + exp(-tmp0 * xx0) * tmp0) / (exp(tmp0) - exp(-tmp0));
   }
   __host__ __device__ void to_cart(double xx0, double xx1, double xx2, double out[3]) const {
+    if (cylindrical()) {
+      // the generated xx_to_Cart (SinhCylindrical)
+      const double tmp0 = (1.0 / (cyl.SINHWRHO));
+      const double tmp3 = (1.0 / (cyl.SINHWZ));
+      const double tmp2 = cyl.AMPLRHO * (exp(tmp0 * xx0) - exp(-tmp0 * xx0)) / (exp(tmp0) - exp(-tmp0));
+      out[0] = tmp2 * cos(xx1);
+      out[1] = tmp2 * sin(xx1);
+      out[2] = cyl.AMPLZ * (exp(tmp3 * xx2) - exp(-tmp3 * xx2)) / (exp(tmp3) - exp(-tmp3));
+      return;
+    }
     const double rr = r(xx0);
     const double tmp = rr * sin(xx1);
     out[0] = tmp * cos(xx2);
@@ -86,11 +107,13 @@ struct Coord {
 };
 
 static int coord_of(const params_struct *p, Coord *c) {
-  if (p->CoordSystem_hash == SPHERICAL) *c = Coord{0, 0.0, 0.0};
-  else if (p->CoordSystem_hash == SINHSPHERICAL) *c = Coord{1, p->AMPL, p->SINHW};
+  *c = Coord{};
+  if (p->CoordSystem_hash == SPHERICAL) c->kind = COORD_SPHERICAL;
+  else if (p->CoordSystem_hash == SINHSPHERICAL) *c = Coord{COORD_SINHSPHERICAL, p->AMPL, p->SINHW, CylMap{}};
+  else if (p->CoordSystem_hash == SINHCYLINDRICAL) *c = Coord{COORD_SINHCYLINDRICAL, 0.0, 0.0, cyl_map(p)};
   else {
-    set_error("CoordSystem_hash %d: only Spherical (%d) and SinhSpherical (%d) are supported",
-              p->CoordSystem_hash, SPHERICAL, SINHSPHERICAL);
+    set_error("CoordSystem_hash %d: only Spherical (%d), SinhSpherical (%d) and SinhCylindrical (%d) are supported",
+              p->CoordSystem_hash, SPHERICAL, SINHSPHERICAL, SINHCYLINDRICAL);
     return BSSN_B200_EINVAL;
   }
   return BSSN_B200_OK;
@@ -110,16 +133,18 @@ int grid_params(const commondata_struct *cd, params_struct *p, REAL *xx[3], cons
   Coord c;
   BSSN_TRY(coord_of(p, &c));
   // Default resolution of the generated project (two_blackholes_collide's Nxx_dict for
-  // Spherical and SinhSpherical), replaced by Nx when all three entries are set.
-  p->Nxx0 = 72;
-  p->Nxx1 = 12;
-  p->Nxx2 = 2;
+  // Spherical and SinhSpherical, blackhole_spectroscopy's for SinhCylindrical), replaced by
+  // Nx when all three entries are set.
+  p->Nxx0 = c.cylindrical() ? 400 : 72;
+  p->Nxx1 = c.cylindrical() ? 2 : 12;
+  p->Nxx2 = c.cylindrical() ? 1200 : 2;
   if (Nx != nullptr && Nx[0] != -1 && Nx[1] != -1 && Nx[2] != -1) {
     p->Nxx0 = Nx[0];
     p->Nxx1 = Nx[1];
     p->Nxx2 = Nx[2];
   }
-  snprintf(p->CoordSystemName, 100, "%s", c.sinh ? "SinhSpherical" : "Spherical");
+  snprintf(p->CoordSystemName, 100, "%s",
+           c.kind == COORD_SPHERICAL ? "Spherical" : (c.cylindrical() ? "SinhCylindrical" : "SinhSpherical"));
   if (apply_defaults) {
     if (p->Nxx0 != 2) p->Nxx0 *= cd->convergence_factor;
     if (p->Nxx1 != 2) p->Nxx1 *= cd->convergence_factor;
@@ -138,15 +163,28 @@ int grid_params(const commondata_struct *cd, params_struct *p, REAL *xx[3], cons
     set_error("grid: %lld points x %d gridfunctions exceeds 32-bit indexing", ntot, NUM_EVOL_GFS);
     return BSSN_B200_EINVAL;
   }
-  if (c.sinh) p->AMPL = p->grid_physical_size;
-  else p->RMAX = p->grid_physical_size;
-  if (apply_defaults) {
-    p->xxmin0 = 0;
-    p->xxmin1 = 0;
-    p->xxmin2 = -p->PI;
-    p->xxmax0 = c.sinh ? 1 : p->RMAX;
-    p->xxmax1 = p->PI;
-    p->xxmax2 = p->PI;
+  if (c.cylindrical()) {
+    p->AMPLRHO = p->grid_physical_size;
+    p->AMPLZ = p->grid_physical_size;
+    if (apply_defaults) {
+      p->xxmin0 = 0;
+      p->xxmin1 = -p->PI;
+      p->xxmin2 = -1;
+      p->xxmax0 = 1;
+      p->xxmax1 = p->PI;
+      p->xxmax2 = 1;
+    }
+  } else {
+    if (c.kind == COORD_SINHSPHERICAL) p->AMPL = p->grid_physical_size;
+    else p->RMAX = p->grid_physical_size;
+    if (apply_defaults) {
+      p->xxmin0 = 0;
+      p->xxmin1 = 0;
+      p->xxmin2 = -p->PI;
+      p->xxmax0 = c.kind == COORD_SINHSPHERICAL ? 1 : p->RMAX;
+      p->xxmax1 = p->PI;
+      p->xxmax2 = p->PI;
+    }
   }
   p->dxx0 = (p->xxmax0 - p->xxmin0) / ((REAL)p->Nxx0);
   p->dxx1 = (p->xxmax1 - p->xxmin1) / ((REAL)p->Nxx1);
@@ -169,7 +207,10 @@ int grid_params(const commondata_struct *cd, params_struct *p, REAL *xx[3], cons
 
 // ---------------------------------------------------------------- rfm precompute (rfm_precompute.py:84-565)
 int rfm_malloc(const params_struct *p, rfm_struct *r) {
-  const size_t n0 = p->Nxx_plus_2NGHOSTS0, n1 = p->Nxx_plus_2NGHOSTS1;
+  // The second function of the reference metric is f1(xx1) in the Spherical family and
+  // f3(xx2) for SinhCylindrical (same rfm_struct slots).
+  const size_t n0 = p->Nxx_plus_2NGHOSTS0,
+               n1 = p->CoordSystem_hash == SINHCYLINDRICAL ? p->Nxx_plus_2NGHOSTS2 : p->Nxx_plus_2NGHOSTS1;
   BSSN_CUDA_TRY(cudaMalloc(&r->f0_of_xx0, sizeof(double) * n0));
   BSSN_CUDA_TRY(cudaMalloc(&r->f0_of_xx0__D0, sizeof(double) * n0));
   BSSN_CUDA_TRY(cudaMalloc(&r->f0_of_xx0__DD00, sizeof(double) * n0));
@@ -194,11 +235,23 @@ int rfm_defines(const params_struct *p, rfm_struct *r, REAL *xx[3]) {
   BSSN_TRY(coord_of(p, &c));
   std::vector<double> hx[3];
   BSSN_TRY(host_xx(p, xx, hx));
-  const int n0 = p->Nxx_plus_2NGHOSTS0, n1 = p->Nxx_plus_2NGHOSTS1;
+  const int n0 = p->Nxx_plus_2NGHOSTS0, n1 = c.cylindrical() ? p->Nxx_plus_2NGHOSTS2 : p->Nxx_plus_2NGHOSTS1;
   std::vector<double> f0(n0), f0d(n0), f0dd(n0), f0ddd(n0), f1(n1), f1d(n1), f1dd(n1);
   for (int i = 0; i < n0; i++) {
     const double xx0 = hx[0][i];
-    if (c.sinh) {
+    if (c.cylindrical()) {
+      const double AMPLRHO = c.cyl.AMPLRHO, SINHWRHO = c.cyl.SINHWRHO;
+      // Expression trees of the generated rfm_precompute_defines (SinhCylindrical).
+      f0[i] = AMPLRHO * (exp(xx0 / SINHWRHO) - exp(-xx0 / SINHWRHO)) / (exp((1.0 / (SINHWRHO))) - exp(-1 / SINHWRHO));
+      f0d[i] = AMPLRHO * (exp(xx0 / SINHWRHO) / SINHWRHO + exp(-xx0 / SINHWRHO) / SINHWRHO) /
+               (exp((1.0 / (SINHWRHO))) - exp(-1 / SINHWRHO));
+      f0dd[i] = AMPLRHO * (exp(xx0 / SINHWRHO) / ((SINHWRHO) * (SINHWRHO)) - exp(-xx0 / SINHWRHO) / ((SINHWRHO) * (SINHWRHO))) /
+                (exp((1.0 / (SINHWRHO))) - exp(-1 / SINHWRHO));
+      f0ddd[i] = AMPLRHO *
+                 (exp(xx0 / SINHWRHO) / ((SINHWRHO) * (SINHWRHO) * (SINHWRHO)) +
+                  exp(-xx0 / SINHWRHO) / ((SINHWRHO) * (SINHWRHO) * (SINHWRHO))) /
+                 (exp((1.0 / (SINHWRHO))) - exp(-1 / SINHWRHO));
+    } else if (c.kind == COORD_SINHSPHERICAL) {
       const double AMPL = c.AMPL, SINHW = c.SINHW;
       // Expression trees of the generated rfm_precompute_defines (SinhSpherical).
       f0[i] = AMPL * (exp(xx0 / SINHW) - exp(-xx0 / SINHW)) / (exp((1.0 / (SINHW))) - exp(-1 / SINHW));
@@ -215,6 +268,19 @@ int rfm_defines(const params_struct *p, rfm_struct *r, REAL *xx[3]) {
     }
   }
   for (int i = 0; i < n1; i++) {
+    if (c.cylindrical()) {
+      // f3_of_xx2 = dz/dxx2 and its two derivatives (the rescaled metric needs z', not z).
+      const double xx2 = hx[2][i], AMPLZ = c.cyl.AMPLZ, SINHWZ = c.cyl.SINHWZ;
+      f1[i] = AMPLZ * (exp(xx2 / SINHWZ) / SINHWZ + exp(-xx2 / SINHWZ) / SINHWZ) /
+              (exp((1.0 / (SINHWZ))) - exp(-1 / SINHWZ));
+      f1d[i] = AMPLZ * (exp(xx2 / SINHWZ) / ((SINHWZ) * (SINHWZ)) - exp(-xx2 / SINHWZ) / ((SINHWZ) * (SINHWZ))) /
+               (exp((1.0 / (SINHWZ))) - exp(-1 / SINHWZ));
+      f1dd[i] = AMPLZ *
+                (exp(xx2 / SINHWZ) / ((SINHWZ) * (SINHWZ) * (SINHWZ)) +
+                 exp(-xx2 / SINHWZ) / ((SINHWZ) * (SINHWZ) * (SINHWZ))) /
+                (exp((1.0 / (SINHWZ))) - exp(-1 / SINHWZ));
+      continue;
+    }
     const double xx1 = hx[1][i];
     f1[i] = sin(xx1);
     f1d[i] = cos(xx1);
@@ -232,21 +298,29 @@ int rfm_defines(const params_struct *p, rfm_struct *r, REAL *xx[3]) {
 
 // ---------------------------------------------------------------- bcstruct (bcstruct_set_up.py:442-792)
 // Eigen-coordinate map of a ghost point (EigenCoord_set_x0x1x2_inbounds__i0i1i2_inbounds_single_pt):
-// (x0,x1,x2) -> Cartesian (eigen-coordinate Spherical) -> (x0,x1,x2)' -> nearest index.
+// (x0,x1,x2) -> Cartesian in the eigen-coordinate system (Spherical for the Spherical family,
+// Cylindrical for SinhCylindrical) -> (x0,x1,x2)' -> nearest index.
 static int eigen_map(const params_struct *p, const Coord &c, const std::vector<double> hx[3], int i0, int i1,
                      int i2, double xin[3], int iin[3]) {
   const double xx0 = hx[0][i0], xx1 = hx[1][i1], xx2 = hx[2][i2];
-  double Cartx, Carty, Cartz;
-  {
+  double Cartx, Carty, Cartz, x0in, x1in, x2in;
+  if (c.cylindrical()) {
+    Cartx = xx0 * cos(xx1);
+    Carty = xx0 * sin(xx1);
+    Cartz = xx2;
+    x0in = sqrt(((Cartx) * (Cartx)) + ((Carty) * (Carty)));
+    x1in = atan2(Carty, Cartx);
+    x2in = Cartz;
+  } else {
     const double tmp0 = xx0 * sin(xx1);
     Cartx = tmp0 * cos(xx2);
     Carty = tmp0 * sin(xx2);
     Cartz = xx0 * cos(xx1);
+    const double tmp1 = sqrt(((Cartx) * (Cartx)) + ((Carty) * (Carty)) + ((Cartz) * (Cartz)));
+    x0in = tmp1;
+    x1in = acos(Cartz / tmp1);
+    x2in = atan2(Carty, Cartx);
   }
-  const double tmp0 = sqrt(((Cartx) * (Cartx)) + ((Carty) * (Carty)) + ((Cartz) * (Cartz)));
-  const double x0in = tmp0;
-  const double x1in = acos(Cartz / tmp0);
-  const double x2in = atan2(Carty, Cartx);
   const double dxx[3] = {p->dxx0, p->dxx1, p->dxx2};
   const double xxmin[3] = {hx[0][0] - ((double)(0 - NGHOSTS) + (1.0 / 2.0)) * dxx[0],
                            hx[1][0] - ((double)(0 - NGHOSTS) + (1.0 / 2.0)) * dxx[1],
@@ -275,7 +349,29 @@ static int eigen_map(const params_struct *p, const Coord &c, const std::vector<d
   return BSSN_B200_OK;
 }
 
-// Unit-vector dot products of the 10 parity types (set_parity_for_inner_boundary_single_pt).
+// Unit-vector dot products of the 10 parity types (set_parity_for_inner_boundary_single_pt):
+// rank-0, the three vector components and the six rank-2 components in the rfm basis.
+static int check_parity(const double par[10], int8_t parity[10]) {
+  const double EPS_REL = 1e-8;
+  for (int k = 0; k < 10; k++) {
+    if (fabs(par[k]) < 1 - EPS_REL || fabs(par[k]) > 1 + EPS_REL) {
+      set_error("bcstruct: parity type %d evaluated to %e, not +/-1", k, par[k]);
+      return BSSN_B200_ESETUP;
+    }
+    parity[k] = par[k] < 0 ? -1 : 1;
+  }
+  return BSSN_B200_OK;
+}
+
+// Cylindrical eigen-coordinates: rho-hat and phi-hat rotate by the phi difference, z-hat is fixed.
+static int parity_signs_cyl(double xx1, const double xin[3], int8_t parity[10]) {
+  const double xx1_inbounds = xin[1];
+  const double tmp0 = sin(xx1) * sin(xx1_inbounds) + cos(xx1) * cos(xx1_inbounds);
+  const double tmp1 = ((tmp0) * (tmp0));
+  const double par[10] = {1, tmp0, tmp0, 1, tmp1, tmp1, tmp0, tmp1, tmp0, 1};
+  return check_parity(par, parity);
+}
+
 static int parity_signs(double xx1, double xx2, const double xin[3], int8_t parity[10]) {
   const double xx1_inbounds = xin[1], xx2_inbounds = xin[2];
   const double tmp0 = cos(xx1) * cos(xx1_inbounds);
@@ -286,15 +382,7 @@ static int parity_signs(double xx1, double xx2, const double xin[3], int8_t pari
   const double tmp5 = tmp0 * tmp2 + tmp0 * tmp3 + tmp1;
   const double tmp6 = tmp2 + tmp3;
   const double par[10] = {1, tmp4, tmp5, tmp6, tmp4 * tmp4, tmp4 * tmp5, tmp4 * tmp6, tmp5 * tmp5, tmp5 * tmp6, tmp6 * tmp6};
-  const double EPS_REL = 1e-8;
-  for (int k = 0; k < 10; k++) {
-    if (fabs(par[k]) < 1 - EPS_REL || fabs(par[k]) > 1 + EPS_REL) {
-      set_error("bcstruct: parity type %d evaluated to %e, not +/-1", k, par[k]);
-      return BSSN_B200_ESETUP;
-    }
-    parity[k] = par[k] < 0 ? -1 : 1;
-  }
-  return BSSN_B200_OK;
+  return check_parity(par, parity);
 }
 
 struct HostBc {
@@ -324,7 +412,8 @@ int bcstruct_host(const params_struct *p, const std::vector<double> hx[3], HostB
         memset(&bc, 0, sizeof(bc));
         bc.dstpt = i0 + N0 * (i1 + N1 * i2);
         bc.srcpt = iin[0] + N0 * (iin[1] + N1 * iin[2]);
-        BSSN_TRY(parity_signs(hx[1][i1], hx[2][i2], xin, bc.parity));
+        if (c.cylindrical()) BSSN_TRY(parity_signs_cyl(hx[1][i1], xin, bc.parity));
+        else BSSN_TRY(parity_signs(hx[1][i1], hx[2][i2], xin, bc.parity));
         out->inner.push_back(bc);
       }
   out->info.num_inner_boundary_points = (int)out->inner.size();
@@ -430,9 +519,20 @@ int cfl_dt(commondata_struct *cd, const params_struct *p, REAL *xx[3]) {
   for (int i2 = 0; i2 < p->Nxx_plus_2NGHOSTS2; i2++)
     for (int i1 = 0; i1 < p->Nxx_plus_2NGHOSTS1; i1++)
       for (int i0 = 0; i0 < p->Nxx_plus_2NGHOSTS0; i0++) {
-        const double xx0 = hx[0][i0], xx1 = hx[1][i1];
+        const double xx0 = hx[0][i0], xx1 = hx[1][i1], xx2 = hx[2][i2];
         double ds0, ds1, ds2;
-        if (c.sinh) {
+        if (c.cylindrical()) {
+          // ds_min_single_pt (SinhCylindrical): dxx0 rho', dxx1 rho, dxx2 z'.
+          const double tmp0 = (1.0 / (c.cyl.SINHWRHO));
+          const double tmp5 = (1.0 / (c.cyl.SINHWZ));
+          const double tmp4 = c.cyl.AMPLRHO / (exp(tmp0) - exp(-tmp0));
+          const double tmp2 = exp(tmp0 * xx0);
+          const double tmp3 = exp(-tmp0 * xx0);
+          ds0 = fabs(p->dxx0 * tmp4 * (tmp0 * tmp2 + tmp0 * tmp3));
+          ds1 = fabs(p->dxx1 * tmp4 * (tmp2 - tmp3));
+          ds2 = fabs(c.cyl.AMPLZ * p->dxx2 * (tmp5 * exp(tmp5 * xx2) + tmp5 * exp(-tmp5 * xx2)) /
+                     (exp(tmp5) - exp(-tmp5)));
+        } else if (c.kind == COORD_SINHSPHERICAL) {
           const double tmp0 = (1.0 / (c.SINHW));
           const double tmp4 = c.AMPL / (exp(tmp0) - exp(-tmp0));
           const double tmp2 = exp(tmp0 * xx0);
@@ -490,13 +590,34 @@ __global__ void bl_initial_data_kernel(const GridDims g, const Coord c, const do
   const double alpha = 1.0 / sqrt(cbrt(detg));
   const double gbar = psi4 * cbrt(1.0 / detg);  // diagonal of gammabar_ij (= 1 up to rounding)
   const double cf = 1.0 / sqrt(cbrt(detg));
-  const double rr = c.r(a0), dr = c.drdx0(a0);
-  const double st = sin(a1), ct = cos(a1), sp_ = sin(a2), cp = cos(a2);
-  const double J[3][3] = {{dr * st * cp, rr * ct * cp, -rr * st * sp_},
-                          {dr * st * sp_, rr * ct * sp_, rr * st * cp},
-                          {dr * ct, -rr * st, 0.0}};
-  const double sf[3] = {dr, rr, rr * st};  // scale factors; ReDD_ij = sf_i sf_j
-  const double ghat[3] = {dr * dr, rr * rr, rr * rr * st * st};
+  // Jacobian d Cart^a / d xx^i of the reference basis and its scale factors (ReDD_ij = sf_i sf_j,
+  // ghat_ii = sf_i^2).
+  double J[3][3], sf[3], ghat[3];
+  if (c.cylindrical()) {
+    const double rho = c.cyl.rho(a0), drho = c.cyl.drho(a0), dz = c.cyl.dz(a2);
+    const double sp_ = sin(a1), cp = cos(a1);
+    const double Jc[3][3] = {{drho * cp, -rho * sp_, 0.0}, {drho * sp_, rho * cp, 0.0}, {0.0, 0.0, dz}};
+    memcpy(J, Jc, sizeof(J));
+    sf[0] = drho;
+    sf[1] = rho;
+    sf[2] = dz;
+    ghat[0] = drho * drho;
+    ghat[1] = rho * rho;
+    ghat[2] = dz * dz;
+  } else {
+    const double rr = c.r(a0), dr = c.drdx0(a0);
+    const double st = sin(a1), ct = cos(a1), sp_ = sin(a2), cp = cos(a2);
+    const double Js[3][3] = {{dr * st * cp, rr * ct * cp, -rr * st * sp_},
+                             {dr * st * sp_, rr * ct * sp_, rr * st * cp},
+                             {dr * ct, -rr * st, 0.0}};
+    memcpy(J, Js, sizeof(J));
+    sf[0] = dr;
+    sf[1] = rr;
+    sf[2] = rr * st;
+    ghat[0] = dr * dr;
+    ghat[1] = rr * rr;
+    ghat[2] = rr * rr * st * st;
+  }
   const size_t n = (size_t)g.ntot;
 #pragma unroll
   for (int gf = 0; gf < NUM_EVOL_GFS; gf++) y[gf * n + idx] = 0.0;

@@ -23,12 +23,14 @@ def _ptr(t: torch.Tensor):
 
 
 class BSSNGrid:
-    """One single-patch Spherical or SinhSpherical grid with RK4 storage on the GPU.
+    """One single-patch Spherical, SinhSpherical or SinhCylindrical grid with RK4 storage on the GPU.
 
     Arguments follow the reference's CodeParameters: ``Nxx`` interior points per
     direction, ``grid_physical_size`` (RMAX for Spherical, AMPL for SinhSpherical),
-    ``SINHW``, Brill-Lindquist masses / z positions, ``CFL_FACTOR``, ``outer_bc_type``
-    ("radiation" or "extrapolation") and ``symmetry_axes`` ("" or "2").
+    ``SINHW`` (SinhSpherical; for SinhCylindrical the width along both rho and z),
+    Brill-Lindquist masses / z positions, ``CFL_FACTOR``, ``outer_bc_type``
+    ("radiation" or "extrapolation") and ``symmetry_axes`` ("" or "2" for the Spherical
+    family; "1" for SinhCylindrical, which is built axisymmetric only).
     """
 
     def __init__(
@@ -71,6 +73,7 @@ class BSSNGrid:
         p.CoordSystem_hash = L.COORD_HASH[coord]
         p.grid_physical_size = grid_physical_size
         p.SINHW = SINHW
+        p.SINHWRHO = p.SINHWZ = SINHW  # SinhCylindrical: the same width along rho and z
         p.grid_idx = 0
         p.gridname = f"grid_{coord}".encode()
         Nx = (C.c_int * 3)(*Nxx)
@@ -135,9 +138,13 @@ class BSSNGrid:
         return [self.device_array(self.gd[0].xx[d], self.N[d]) for d in range(3)]
 
     def rfm(self) -> Dict[str, np.ndarray]:
+        """Host copies of the rfm precompute arrays: the f0 family over xx0; the second family
+        over xx1 (Spherical family: sin(xx1) and derivatives) or, for SinhCylindrical, over xx2
+        (z'(xx2) and derivatives, the generated project's f3_of_xx2 arrays)."""
         out = {}
+        second = 2 if self.coord == "SinhCylindrical" else 1
         for name, _ in L.RfmStruct._fields_:
-            n = self.N[0] if name.startswith("f0") else self.N[1]
+            n = self.N[0] if name.startswith("f0") else self.N[second]
             out[name] = self.device_array(getattr(self._rfm, name), n)
         return out
 

@@ -29,7 +29,8 @@ TOTAL_NUM_DIAG_GFS = len(DIAG_GFS)
 MAXNUMGRIDS = 15
 SPHERICAL = 1307621703
 SINHSPHERICAL = 579707936
-COORD_HASH = {"Spherical": SPHERICAL, "SinhSpherical": SINHSPHERICAL}
+SINHCYLINDRICAL = 1325205359
+COORD_HASH = {"Spherical": SPHERICAL, "SinhSpherical": SINHSPHERICAL, "SinhCylindrical": SINHCYLINDRICAL}
 
 GF_NAMES = [
     "aDD00", "aDD01", "aDD02", "aDD11", "aDD12", "aDD22", "alpha", "betU0", "betU1", "betU2",
@@ -74,8 +75,9 @@ class CheckpointCommondata(C.Structure):
 
 class ParamsStruct(C.Structure):
     _fields_ = [
-        ("AMPL", REAL), ("Cart_originx", REAL), ("Cart_originy", REAL), ("Cart_originz", REAL),
-        ("PI", REAL), ("RMAX", REAL), ("SINHW", REAL), ("dxx0", REAL), ("dxx1", REAL), ("dxx2", REAL),
+        ("AMPL", REAL), ("AMPLRHO", REAL), ("AMPLZ", REAL), ("Cart_originx", REAL), ("Cart_originy", REAL),
+        ("Cart_originz", REAL), ("PI", REAL), ("RHOMAX", REAL), ("RMAX", REAL), ("SINHW", REAL), ("SINHWRHO", REAL),
+        ("SINHWZ", REAL), ("ZMAX", REAL), ("ZMIN", REAL), ("dxx0", REAL), ("dxx1", REAL), ("dxx2", REAL),
         ("grid_hole_radius", REAL), ("grid_physical_size", REAL), ("invdxx0", REAL), ("invdxx1", REAL),
         ("invdxx2", REAL), ("xmax", REAL), ("xmin", REAL), ("xxmax0", REAL), ("xxmax1", REAL),
         ("xxmax2", REAL), ("xxmin0", REAL), ("xxmin1", REAL), ("xxmin2", REAL), ("ymax", REAL),

@@ -23,6 +23,9 @@ Variants
   sph3dck: sph3d plus write_checkpoint/read_checkpoint (checkpoint file parity)
   sph3d8, sinh3d8, sphaxi8: sph3d, sinh3d and sphaxi with 8th-order finite differences
            (NGHOSTS = 5)
+  sinhaxi, sinhaxi8: SinhSpherical, symmetry_axes="2", 4th and 8th order
+  sinhcyl, sinhcyl8: SinhCylindrical, symmetry_axes="1" (axisymmetric about z), 4th and
+           8th order; blackhole_spectroscopy's coordinates (its project uses fd_order 8)
   sinh3d_cuda: sinh3d emitted by the reference's CUDA path (``--cuda``), compiled with nvcc
            for sm_100a (relocatable device code, the generated Makefile's flags with
            ``-arch=sm_100a``) together with ``oracle/ref_harness_cuda.cu`` into
@@ -51,6 +54,10 @@ VARIANTS = {
     "sph3d8": ["--coord", "Spherical", "--fd-order", "8"],
     "sinh3d8": ["--coord", "SinhSpherical", "--fd-order", "8"],
     "sphaxi8": ["--coord", "Spherical", "--axisym", "--fd-order", "8"],
+    "sinhaxi": ["--coord", "SinhSpherical", "--axisym"],
+    "sinhaxi8": ["--coord", "SinhSpherical", "--axisym", "--fd-order", "8"],
+    "sinhcyl": ["--coord", "SinhCylindrical", "--axisym"],
+    "sinhcyl8": ["--coord", "SinhCylindrical", "--axisym", "--fd-order", "8"],
 }
 # Variants emitted by the reference's CUDA path (built with nvcc; not in the default list).
 CUDA_VARIANTS = {

@@ -36,10 +36,15 @@ ref_sim *ref_create(const int Nx0, const int Nx1, const int Nx2, const double gr
   params_struct *params = &g->params;
   params->grid_physical_size = grid_physical_size;
   params->SINHW = sinhw;
+  params->SINHWRHO = sinhw;
+  params->SINHWZ = sinhw;
   params->grid_idx = 0;
   const int Nx[3] = {Nx0, Nx1, Nx2};
   // CoordSystem hash: each generated project contains exactly one CoordSystem.
-#ifdef SINHSPHERICAL
+#if defined(SINHCYLINDRICAL)
+  params->CoordSystem_hash = SINHCYLINDRICAL;
+  snprintf(params->gridname, 100, "grid_SinhCylindrical");
+#elif defined(SINHSPHERICAL)
   params->CoordSystem_hash = SINHSPHERICAL;
   snprintf(params->gridname, 100, "grid_SinhSpherical");
 #else

@@ -19,9 +19,10 @@ nrpy/examples/two_blackholes_collide.py:60-440 with the settings the workloads n
   which adds the REAL CodeParameter checkpoint_every to commondata_struct;
 * ``--fd-order N`` sets the interior finite-difference order (4 by default; NGHOSTS = N/2 + 1),
   the outer radiation condition staying at radiation_BC_fd_order = 4;
-* the reference metrics of Spherical, SinhSpherical and SinhCylindrical are all instantiated,
-  so that every variant's params_struct carries the CodeParameters of all three and one
-  layout serves every project variant.
+* the reference metrics of Spherical, SinhSpherical, SinhCylindrical and Cylindrical (the
+  eigen-coordinates of SinhCylindrical, whose bcstruct set-up instantiates it) are all
+  instantiated, so that every variant's params_struct carries the CodeParameters of all four
+  and one layout serves every project variant.
 
 Run it with the reference on PYTHONPATH (oracle/gen_ref.py does this).
 """
@@ -53,7 +54,7 @@ par.set_parval_from_str("fp_type", "double")
 CoordSystem = args.coord
 set_of_CoordSystems = {CoordSystem}
 grid_physical_size = 7.5 if CoordSystem == "Spherical" else 10.0
-Nxx_dict = {"Spherical": [72, 12, 2], "SinhSpherical": [256, 64, 64], "SinhCylindrical": [128, 2, 256]}
+Nxx_dict = {"Spherical": [72, 12, 2], "SinhSpherical": [256, 64, 64], "SinhCylindrical": [400, 2, 1200]}
 OMP_collapse = 2
 if args.axisym:
     par.set_parval_from_str("symmetry_axes", "1" if "Cylindrical" in CoordSystem else "2")
@@ -66,7 +67,7 @@ par.set_parval_from_str("CoordSystem_to_register_CodeParameters", "All")
 # Instantiate both reference metrics so that both register their CodeParameters
 # (RMAX for Spherical; AMPL, SINHW for SinhSpherical): every variant then shares one
 # params_struct layout.
-for _coord in ("Spherical", "SinhSpherical", "SinhCylindrical"):
+for _coord in ("Spherical", "SinhSpherical", "SinhCylindrical", "Cylindrical"):
     _ = refmetric.reference_metric[_coord]
 
 if parallelization == "cuda":

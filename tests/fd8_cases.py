@@ -1,5 +1,5 @@
 """8th-order finite differences (libbssn_b200_fd8.so, NGHOSTS = 5) against the reference's own
-generated C at fd_order = 8 (oracle variants sph3d8, sinh3d8). B200.
+generated C at fd_order = 8 (oracle variants sph3d8, sinh3d8, sphaxi8, sinhaxi8, sinhcyl8). B200.
 
 Not collected by the main test run: the library's finite-difference order is fixed per
 process (BSSN_B200_FD_ORDER, read when nrpy_b200.lib is imported), so test_fd8_gpu.py runs
@@ -17,6 +17,14 @@ import torch
 
 from oracle import ref as oref
 from tests.util import rel_l2_per_gf
+
+from tests.sinhaxi_cases import test_sinhaxi_20_steps, test_sinhaxi_ricci_rhs  # noqa: F401  (oracle sinhaxi8)
+from tests.sinhcyl_cases import (  # noqa: F401  (SinhCylindrical at 8th order: oracle variant sinhcyl8)
+    test_sinhcyl_20_steps,
+    test_sinhcyl_brill_lindquist_50_steps,
+    test_sinhcyl_grid_bcstruct_and_initial_data,
+    test_sinhcyl_ricci_rhs_constraints,
+)
 
 pytestmark = pytest.mark.gpu
 G = 5

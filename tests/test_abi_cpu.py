@@ -61,14 +61,15 @@ def test_struct_layouts_match_reference_project():
         "offsetof_commondata_nn": L.CommondataStruct.nn.offset,
     }
     # Layout of the reference's generated BHaH_defines.h (x86-64), from oracle/ref_harness.c.
-    expected = {"sizeof_commondata": 232, "sizeof_params": 456, "sizeof_bc_struct": 552, "sizeof_griddata": 1080,
-                "sizeof_innerpt": 20, "sizeof_outerpt": 10, "offsetof_params_Nxx0": 424,
-                "offsetof_params_invdxx0": 96, "offsetof_params_hash": 420, "offsetof_commondata_eta": 112,
+    # Its params_struct carries the CodeParameters of Spherical, SinhSpherical and SinhCylindrical.
+    expected = {"sizeof_commondata": 232, "sizeof_params": 512, "sizeof_bc_struct": 552, "sizeof_griddata": 1136,
+                "sizeof_innerpt": 20, "sizeof_outerpt": 10, "offsetof_params_Nxx0": 480,
+                "offsetof_params_invdxx0": 152, "offsetof_params_hash": 476, "offsetof_commondata_eta": 112,
                 "offsetof_commondata_dt": 104, "offsetof_commondata_bc": 160, "offsetof_commondata_nn": 216}
     assert mine == expected
     from oracle import ref
 
-    for variant in ("sphaxi", "sph3d", "sinh3d"):
+    for variant in ("sphaxi", "sph3d", "sinh3d", "sinhcyl"):
         if ref.available(variant):
             assert ref.struct_layout(variant) == expected
 
@@ -76,6 +77,8 @@ def test_struct_layouts_match_reference_project():
 def test_symmetry_setting_validation():
     lib = L.load()
     assert lib.bssn_b200_set_symmetry_axes(b"2") == 0
+    assert lib.bssn_b200_set_symmetry_axes(b"") == 0
+    assert lib.bssn_b200_set_symmetry_axes(b"1") == 0  # SinhCylindrical, axisymmetric about z
     assert lib.bssn_b200_set_symmetry_axes(b"") == 0
     assert lib.bssn_b200_set_symmetry_axes(b"01") == -1
     assert b"only" in lib.bssn_b200_last_error()

@@ -12,6 +12,7 @@ import pytest
 import torch
 
 from oracle import ref as oref
+from tests.sinhaxi_cases import test_sinhaxi_20_steps, test_sinhaxi_ricci_rhs  # noqa: F401  (oracle sinhaxi)
 from tests.util import as4, interior, rel_l2_per_gf
 
 pytestmark = pytest.mark.gpu
