@@ -418,7 +418,7 @@ def main():
         y_cmp = mixed.pop("_y_cmp", None) if mixed else None
         if not args.no_cpu_baseline:
             try:
-                cpu = cpu_reference_rate(3, 2, 3, args.seed)
+                cpu = cpu_reference_rate(3, 5, 3, args.seed)
             except Exception as e:  # noqa: BLE001
                 cpu = {"unavailable": str(e)}
             if mixed is not None and y_cmp is not None:

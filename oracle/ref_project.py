@@ -64,8 +64,9 @@ shutil.rmtree(project_dir, ignore_errors=True)
 par.set_parval_from_str("enable_parallel_codegen", True)
 par.set_parval_from_str("fd_order", args.fd_order)
 par.set_parval_from_str("CoordSystem_to_register_CodeParameters", "All")
-# Instantiate both reference metrics so that both register their CodeParameters
-# (RMAX for Spherical; AMPL, SINHW for SinhSpherical): every variant then shares one
+# Instantiate the four reference metrics so that all register their CodeParameters (RMAX for
+# Spherical; AMPL, SINHW for SinhSpherical; AMPLRHO, AMPLZ, SINHWRHO, SINHWZ for
+# SinhCylindrical; RHOMAX, ZMIN, ZMAX for Cylindrical): every variant then shares one
 # params_struct layout.
 for _coord in ("Spherical", "SinhSpherical", "SinhCylindrical", "Cylindrical"):
     _ = refmetric.reference_metric[_coord]
