@@ -616,12 +616,11 @@ def run_batched(args, world, rank, dist):
     be = BatchedEvolutions([specs[i] for i in mine])
     if args.batch_tile:
         bx, by = (int(x) for x in args.batch_tile.split(","))
-        tune = {"tile": (bx, by), "blocks": 4 * torch.cuda.get_device_properties(be.device).multi_processor_count,
-                "table": "not run (--batch-tile)"}
+        tune = {"tile": (bx, by), "table": "not run (--batch-tile)"}
     else:
         tune = be.autotune(steps=2)
     spg = 20
-    be.build(tile=tune["tile"], blocks=tune["blocks"], steps_per_graph=spg)
+    be.build(tile=tune["tile"], steps_per_graph=spg)
     be.run(1)
     torch.cuda.synchronize()
     steps = max(spg, (args.batch_steps // spg) * spg)
@@ -654,7 +653,7 @@ def run_batched(args, world, rank, dist):
     seq_value = aggregate(pts, seq_steps, seq_ms, dist, device="cuda")[0] if seq_ms > 0 else None
     be.close()
     return {"value": value, "unit": UNIT, "evolutions": len(specs), "steps": steps, "ms_per_step": ms_max / steps,
-            "interior_points": pts if dist is None else None, "tile": list(tune["tile"]), "blocks": tune["blocks"],
+            "interior_points": pts if dist is None else None, "tile": list(tune["tile"]),
             "autotune": tune["table"], "graph_kernel_nodes_per_replay": info["kernel_nodes"],
             "tile_fill": info["tile_fill"],
             "sequential_single_grid_value": seq_value,

@@ -376,17 +376,17 @@ int bssn_b200_stepper_kernel_nodes(const bssn_b200_stepper *st, unsigned long lo
 /* Batched evolutions: `nevo` independent grids (each set up through the entry points above:
  * grid, rfm, bcstruct, storage, initial data; all of one coordinate system, full 3-D,
  * radiation outer BCs; each with its own commondata: masses, dt, ...) advanced together.
- * Each RK4 stage of the whole batch takes a fixed number of launches: persistent kernels
- * (`blocks` CTAs) walk one tile list over all grids; a tile is tile_bx x tile_by = 128 points,
- * or, with tile_bx = tile_by = 0, per grid the 128-point brick (i0 x i1 x i2, i0 extent 16
- * to 128) that pads that grid's interior least.
+ * Each RK4 stage of the whole batch takes a fixed number of launches (one per group kernel
+ * for every 120 grids): the Ricci and RHS group kernels run one block per tile over the tiles
+ * of all grids; a tile is tile_bx x tile_by = 128 points, or, with tile_bx = tile_by = 0, per
+ * grid the 128-point brick (i0 x i1 x i2, i0 extent 16 to 128) that pads that grid's
+ * interior least.
  * `steps_per_graph` RK4 steps are captured into a CUDA graph on `stream` (non-default);
  * bssn_b200_batch_run replays it. Creation allocates the per-grid RHS shells and the
  * device work lists; the caller's states are unchanged by it. */
 typedef struct bssn_b200_batch bssn_b200_batch;
 int bssn_b200_batch_create(int nevo, commondata_struct *const *commondatas, griddata_struct *const *griddatas,
-                           int tile_bx, int tile_by, int blocks, int steps_per_graph, void *stream,
-                           bssn_b200_batch **out);
+                           int tile_bx, int tile_by, int steps_per_graph, void *stream, bssn_b200_batch **out);
 int bssn_b200_batch_run(bssn_b200_batch *batch, int graph_launches);
 int bssn_b200_batch_info(const bssn_b200_batch *batch, int *ntiles, int *nouter, int *ninner,
                          unsigned long long *kernel_nodes);

@@ -2,10 +2,10 @@
 
 Each evolution is a full single-patch grid (its own resolution, masses, positions and
 CFL timestep) set up through the C ABI exactly like BSSNGrid; libbssn_b200's batch
-object then advances all of them with a fixed number of launches per RK4 stage
-(persistent kernels over one tile list that spans every grid) and replays the step as a
-captured CUDA graph. The tile shape and the persistent grid size are chosen by
-`autotune`, which times each candidate on the batch itself.
+object then advances all of them with a fixed number of launches per RK4 stage (group
+kernels with one block per 128-point tile over the tiles of every grid) and replays the
+step as a captured CUDA graph. The tile shape is chosen by `autotune`, which times each
+candidate on the batch itself.
 
 Multi-GPU: evolutions are independent, so they shard across ranks with no collective;
 `partition_evolutions` gives the load-balanced split (greedy longest-processing-time by
@@ -65,7 +65,7 @@ class BatchedEvolutions:
         self.device = self.grids[0].device
         self.stream = torch.cuda.Stream(self.device)
         self._batch = None
-        self.config: Optional[Tuple[Tuple[int, int], int]] = None
+        self.config: Optional[Tuple[int, int]] = None
         n = len(self.grids)
         self._cds = (L.PCD * n)(*[C.pointer(g.cd) for g in self.grids])
         self._gds = (L.PGD * n)(*[C.cast(g.gd, L.PGD) for g in self.grids])
@@ -74,20 +74,16 @@ class BatchedEvolutions:
     def interior_points(self) -> int:
         return sum(g.n_interior for g in self.grids)
 
-    def build(self, tile: Tuple[int, int] = PER_GRID, blocks: Optional[int] = None, steps_per_graph: int = 1):
+    def build(self, tile: Tuple[int, int] = PER_GRID, steps_per_graph: int = 1):
         """Create the batch object and capture its graph: `tile` = (bx, by) with bx*by = 128 for
         one shape for every grid, or PER_GRID for a brick chosen per grid."""
-        import torch
-
         self.free()
-        if blocks is None:
-            blocks = 2 * torch.cuda.get_device_properties(self.device).multi_processor_count
         b = C.c_void_p()
-        L.check(self.lib.bssn_b200_batch_create(len(self.grids), self._cds, self._gds, tile[0], tile[1], blocks,
+        L.check(self.lib.bssn_b200_batch_create(len(self.grids), self._cds, self._gds, tile[0], tile[1],
                                                 steps_per_graph, C.c_void_p(self.stream.cuda_stream), C.byref(b)))
         self._batch = b
         self._steps_per_graph = steps_per_graph
-        self.config = (tuple(tile), blocks)
+        self.config = tuple(tile)
 
     def run(self, graph_launches: int) -> None:
         if self._batch is None:
@@ -112,33 +108,30 @@ class BatchedEvolutions:
             g.y_n.copy_(y)
             g.cd.time, g.cd.nn = t, n
 
-    def autotune(self, steps: int = 2, tiles: Sequence[Tuple[int, int]] = TILE_SHAPES,
-                 blocks_per_sm: Sequence[int] = (1, 2, 4)) -> Dict:
-        """Time each (tile shape, persistent grid size) on this batch; keep the fastest.
-        The evolutions' states are restored afterwards."""
+    def autotune(self, steps: int = 2, tiles: Sequence[Tuple[int, int]] = TILE_SHAPES) -> Dict:
+        """Time each tile shape on this batch; keep the fastest. The evolutions' states are
+        restored afterwards."""
         import torch
 
-        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         saved = self.save_states()
         torch.cuda.synchronize()
         results = []
         for tile in tiles:
-            for bps in blocks_per_sm:
-                self.build(tile=tile, blocks=bps * sms, steps_per_graph=1)
-                self.run(1)  # warm-up
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(self.stream)
-                self.run(steps)
-                b.record(self.stream)
-                b.synchronize()
-                results.append((a.elapsed_time(b) / steps, tile, bps * sms))
+            self.build(tile=tile, steps_per_graph=1)
+            self.run(1)  # warm-up
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(self.stream)
+            self.run(steps)
+            b.record(self.stream)
+            b.synchronize()
+            results.append((a.elapsed_time(b) / steps, tile))
         self.restore_states(saved)
         torch.cuda.synchronize()
         results.sort()
         best = results[0]
         self.free()
-        return {"ms_per_step": best[0], "tile": best[1], "blocks": best[2],
-                "table": [{"ms_per_step": r[0], "tile": r[1], "blocks": r[2]} for r in results]}
+        return {"ms_per_step": best[0], "tile": best[1],
+                "table": [{"ms_per_step": r[0], "tile": r[1]} for r in results]}
 
     def free(self) -> None:
         if getattr(self, "_batch", None) is not None:

@@ -90,26 +90,26 @@ struct PointCtx {
 #undef invdxx1
 #undef invdxx2
 constexpr int NG = TUNE_NG, N0 = 256 + 2 * NG, N1 = 64 + 2 * NG, N2 = 32 + 2 * NG, NTOT = N0 * N1 * N2, MAXOUT = 18;
-template <int NT, int MINB, int NOUT, class F>
+template <typename VT, int NT, int MINB, int NOUT, class F>
 __global__ void __launch_bounds__(NT, MINB) kern(RfmArrays rfm, const double *in, const double *aux, double *out) {
   const int i0 = NG + blockIdx.x * 32 + threadIdx.x, i1 = NG + blockIdx.y * (NT / 32) + threadIdx.y, i2 = NG + blockIdx.z;
   if (i0 >= N0 - NG || i1 >= N1 - NG) return;
   extern __shared__ double smem[];
-  volatile double *sm = smem + threadIdx.x + 32 * threadIdx.y;
+  volatile VT *sm = reinterpret_cast<VT *>(smem) + threadIdx.x + 32 * threadIdx.y;
   const int idx = i0 + N0 * i1 + N0 * N1 * i2;
   PointCtx ctx;
   ctx.in = in + idx; ctx.aux = aux + idx; ctx.s1 = N0; ctx.s2 = N0 * N1; ctx.ntot = NTOT; ctx.i0 = i0; ctx.i1 = i1;
   ctx.invdxx0 = 10.0; ctx.invdxx1 = 20.0; ctx.invdxx2 = 5.0; ctx.rfm = rfm; ctx.eta = 1.0;
   ctx.KreissOliger_strength_gauge = 0.3; ctx.KreissOliger_strength_nongauge = 0.3;
-  double o[NOUT];
+  VT o[NOUT];
   F::template eval<NT>(ctx, o, sm);
 #pragma unroll
-  for (int k = 0; k < NOUT; k++) out[idx + k * NTOT] = o[k];
+  for (int k = 0; k < NOUT; k++) out[idx + k * NTOT] = (double)o[k];
 }
-template <int NT, int MINB, int NOUT, int SLOTS, class F>
+template <typename VT, int NT, int MINB, int NOUT, int SLOTS, class F>
 void run(const char *name, RfmArrays rfm, const double *in, const double *aux, double *out) {
-  auto K = kern<NT, MINB, NOUT, F>;
-  const size_t sb = (size_t)SLOTS * NT * 8;
+  auto K = kern<VT, NT, MINB, NOUT, F>;
+  const size_t sb = (size_t)SLOTS * NT * sizeof(VT);
   if (sb > 227 * 1024) { printf("{\"kernel\": \"%s\", \"skip\": \"shared memory\"}\n", name); return; }
   if (cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb) != cudaSuccess) return;
   cudaFuncAttributes at;
@@ -173,14 +173,14 @@ def generate() -> None:
                                            upwind_vec=uv, reg_capacity=cap, remat_first=rf, deriv_remat=dr)
             parts.append(code)
             slots = max(st["smem_slots"], 1)
-            wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
-                            f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
+            wrappers.append(f"struct W_{fname} {{ template <int NT, class C, class VT> __device__ __forceinline__ static void "
+                            f"eval(const C &c, VT *o, volatile VT *sm) {{ {fname}<VT, double, NT>(c, o, sm); }} }};")
             nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
             launches = [(nt, minb)] if minb == 1 else [(128, minb), (64, 2 * minb)]
             if minb == 1 and nt == 128:
                 launches.append((64, 1))
             for t, mb in launches:
-                calls.append(f'  run<{t}, {mb}, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+                calls.append(f'  run<double, {t}, {mb}, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
         (OUT / f"{gname}.cuh").write_text("\n".join(parts))
         head, main = HARNESS_HEAD.replace("GROUP", gname).split("int main() {")
         body = head + "\n".join(wrappers) + "\nint main() {" + main
@@ -213,10 +213,10 @@ def generate_orders() -> None:
                                                order=order)
                 parts.append(code)
                 slots = max(st["smem_slots"], 1)
-                wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
-                                f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
+                wrappers.append(f"struct W_{fname} {{ template <int NT, class C, class VT> __device__ __forceinline__ static void "
+                                f"eval(const C &c, VT *o, volatile VT *sm) {{ {fname}<VT, double, NT>(c, o, sm); }} }};")
                 nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
-                calls.append(f'  run<{nt}, 1, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+                calls.append(f'  run<double, {nt}, 1, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
         tag = f"order_{gname}"
         (OUT / f"{tag}.cuh").write_text("\n".join(parts))
         head, main = HARNESS_HEAD.replace("GROUP", tag).split("int main() {")
@@ -225,13 +225,15 @@ def generate_orders() -> None:
         print(tag, flush=True)
 
 
-def generate_caps(caps, fd_order: int = 4) -> None:
+def generate_caps(caps, fd_order: int = 4, dtype: str = "double") -> None:
     """The present groups with their chosen allocation and order (generate.py) at several
-    register budgets, at the given finite-difference order."""
+    register budgets, at the given finite-difference order, evaluated in `dtype` (double, or
+    float as the mixed-precision kernels run them: FP32 algebra on FP64 finite differences,
+    with the slot qualifier generate.py gives FP32 groups)."""
     from nrpy_b200.codegen import bssn_exprs as be
     from nrpy_b200.codegen import fdcoeffs as fdc
     from nrpy_b200.codegen.emit_cuda import emit_point_function
-    from nrpy_b200.codegen.generate import RHS_ALLOC, RICCI_ALLOC
+    from nrpy_b200.codegen.generate import RHS_ALLOC, RHS_PLAIN_SLOTS, RICCI_ALLOC, RICCI_PLAIN_SLOTS
 
     fdc.set_fd_order(fd_order)
     be.setup_nrpy("", fd_order)
@@ -239,6 +241,8 @@ def generate_caps(caps, fd_order: int = 4) -> None:
     ricci = be.ricci_exprs("SinhSpherical")
     OUT.mkdir(parents=True, exist_ok=True)
     chosen = dict(zip(ORDER_GROUPS, list(RICCI_ALLOC) + list(RHS_ALLOC)))
+    plain = dict(zip(ORDER_GROUPS, [dtype in t for t in list(RICCI_PLAIN_SLOTS) + list(RHS_PLAIN_SLOTS)]))
+    vbytes = 4 if dtype == "float" else 8
     for gname in ORDER_GROUPS:
         kind, names = CANDIDATES[gname]
         src, uv = (ricci, None) if kind == "ricci" else (rhs, betaU)
@@ -250,11 +254,12 @@ def generate_caps(caps, fd_order: int = 4) -> None:
                                            upwind_vec=uv, reg_capacity=cap, remat_first=rf, deriv_remat=dr, order=order)
             parts.append(code)
             slots = max(st["smem_slots"], 1)
-            wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
-                            f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
-            nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
-            calls.append(f'  run<{nt}, 1, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
-        tag = f"caps_{gname}" if fd_order == 4 else f"caps{fd_order}_{gname}"
+            smp = "const_cast<VT *>(sm)" if plain[gname] else "sm"
+            wrappers.append(f"struct W_{fname} {{ template <int NT, class C, class VT> __device__ __forceinline__ static void "
+                            f"eval(const C &c, VT *o, volatile VT *sm) {{ {fname}<VT, double, NT>(c, o, {smp}); }} }};")
+            nt = 128 if 2 * slots * vbytes * 128 <= 227 * 1024 else 64
+            calls.append(f'  run<{dtype}, {nt}, 1, {len(names)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+        tag = (f"caps_{gname}" if fd_order == 4 else f"caps{fd_order}_{gname}") + ("_f32" if dtype == "float" else "")
         (OUT / f"{tag}.cuh").write_text("\n".join(parts))
         head, main = HARNESS_HEAD.replace("GROUP", tag).replace("#define TUNE_NG 3", f"#define TUNE_NG {fdc.NGHOSTS}"
                                                                  ).split("int main() {")
@@ -312,13 +317,13 @@ def generate_leaf() -> None:
                                            reg_capacity=cap, remat_first=rf, deriv_remat=dr, order=order, leaf_index=li)
             parts.append(code)
             slots = max(st["smem_slots"], 1)
-            wrappers.append(f"struct W_{fname} {{ template <int NT, class C> __device__ __forceinline__ static void "
-                            f"eval(const C &c, double *o, volatile double *sm) {{ {fname}<double, double, NT>(c, o, sm); }} }};")
+            wrappers.append(f"struct W_{fname} {{ template <int NT, class C, class VT> __device__ __forceinline__ static void "
+                            f"eval(const C &c, VT *o, volatile VT *sm) {{ {fname}<VT, double, NT>(c, o, sm); }} }};")
             nt = 128 if 2 * slots * 8 * 128 <= 227 * 1024 else 64
-            calls.append(f'  run<{nt}, 1, {len(gn)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
-    wrappers.append("struct W_leaf { template <int NT, class C> __device__ __forceinline__ static void "
-                    "eval(const C &c, double *o, volatile double *sm) { leaf_all<double, double>(c); o[0] = 0.0; } };")
-    calls.append('  run<128, 1, 1, 1, W_leaf>("leaf_all", rfm, in, aux, out);')
+            calls.append(f'  run<double, {nt}, 1, {len(gn)}, {slots}, W_{fname}>("{fname}", rfm, in, aux, out);')
+    wrappers.append("struct W_leaf { template <int NT, class C, class VT> __device__ __forceinline__ static void "
+                    "eval(const C &c, VT *o, volatile VT *sm) { leaf_all<double, double>(c); o[0] = 0.0; } };")
+    calls.append('  run<double, 128, 1, 1, 1, W_leaf>("leaf_all", rfm, in, aux, out);')
     (OUT / "leaf.cuh").write_text("\n".join(parts))
     h, m = head.replace("GROUP", "leaf").split("int main() {")
     n = len(names)
@@ -373,6 +378,7 @@ if __name__ == "__main__":
                                      "summarize"])
     ap.add_argument("--caps", default="72,80,90,100")
     ap.add_argument("--fd-order", type=int, default=4)
+    ap.add_argument("--dtype", default="double", choices=["double", "float"], help="value type of generate-caps")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--log", default=None)
     a = ap.parse_args()
@@ -381,7 +387,7 @@ if __name__ == "__main__":
     elif a.step == "generate-orders":
         generate_orders()
     elif a.step == "generate-caps":
-        generate_caps([int(c) for c in a.caps.split(",")], a.fd_order)
+        generate_caps([int(c) for c in a.caps.split(",")], a.fd_order, a.dtype)
     elif a.step == "generate-leaf":
         generate_leaf()
     elif a.step == "compile":

@@ -1,13 +1,14 @@
 // Many independent BSSN evolutions (uneven grid sizes) advanced together.
 //
 // Every RK4 stage of every evolution runs in a fixed number of launches that each cover
-// the whole batch: persistent kernels walk one tile list spanning all evolutions for the
-// Ricci and fused RHS + RK-update groups, and concatenated point lists serve the outer
-// radiation layers, the RK update of outer points and the inner parity copies. The
-// per-evolution geometry, buffers, timestep and physical parameters sit in a device
-// descriptor array (EvoDesc). `steps_per_graph` RK4 steps are captured once into a CUDA
-// graph and replayed; the tile shape and persistent grid size come from the caller
-// (nrpy_b200.batch autotunes them).
+// the whole batch (up to kChunkEvos evolutions per launch of a Ricci or RHS group kernel):
+// those kernels run one block per 128-point tile over the tiles of all their evolutions,
+// and concatenated point lists serve the outer radiation layers, the RK update of outer
+// points and the inner parity copies. The per-evolution geometry, buffers, timestep and
+// physical parameters are EvoDesc descriptors: by value in the group kernels' parameters
+// (BatchChunk), and as a device array for the boundary kernels. `steps_per_graph` RK4
+// steps are captured once into a CUDA graph and replayed; the tile shape comes from the
+// caller (nrpy_b200.batch autotunes it).
 #include <algorithm>
 #include <cstring>
 #include <vector>
@@ -22,7 +23,7 @@ struct bssn_b200_batch {
   std::vector<commondata_struct *> cds;
   std::vector<griddata_struct *> gds;
   EvoDesc *d_descs = nullptr;
-  int *d_tile_evo = nullptr;
+  std::vector<BatchChunk> chunks;  // the Ricci / RHS launches' parameters
   int ntiles = 0;
   BatchOuterPt *d_outer_layer[NGHOSTS] = {nullptr, nullptr, nullptr};
   int nouter_layer[NGHOSTS] = {0, 0, 0};
@@ -31,7 +32,7 @@ struct bssn_b200_batch {
   BatchInnerPt *d_inner = nullptr;
   int ninner = 0;
   std::vector<double *> krhs;
-  int bx = 32, by = 4, blocks = 296, steps_per_graph = 1;  // bx = by = 0: a tile shape per evolution
+  int bx = 32, by = 4, steps_per_graph = 1;  // bx = by = 0: a tile shape per evolution
   long long padded_points = 0, interior_points = 0;          // tile capacity and interior points covered
   cudaStream_t stream = nullptr;
   cudaGraph_t graph = nullptr;
@@ -42,8 +43,8 @@ struct bssn_b200_batch {
 namespace bssn {
 
 static int batch_stage(bssn_b200_batch *b, int stage, cudaStream_t s) {
-  BSSN_TRY(launch_ricci_batched(b->v, stage, b->d_descs, b->d_tile_evo, b->ntiles, b->blocks, s));
-  BSSN_TRY(launch_rhs_fused_batched(b->v, stage, b->d_descs, b->d_tile_evo, b->ntiles, b->blocks, s));
+  for (const BatchChunk &c : b->chunks) BSSN_TRY(launch_ricci_batched(b->v, stage, c, s));
+  for (const BatchChunk &c : b->chunks) BSSN_TRY(launch_rhs_fused_batched(b->v, stage, c, s));
   for (int gz = 0; gz < NGHOSTS; gz++)
     BSSN_TRY(launch_radiation_batched(stage, b->d_descs, b->d_outer_layer[gz], b->nouter_layer[gz], s));
   BSSN_TRY(launch_rk_points_batched(b->v, stage, b->d_descs, b->d_outer_all, b->nouter_all, s));
@@ -88,7 +89,6 @@ static void batch_free(bssn_b200_batch *b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   cudaFree(b->d_descs);
-  cudaFree(b->d_tile_evo);
   for (int gz = 0; gz < NGHOSTS; gz++) cudaFree(b->d_outer_layer[gz]);
   cudaFree(b->d_outer_all);
   cudaFree(b->d_inner);
@@ -97,7 +97,7 @@ static void batch_free(bssn_b200_batch *b) {
 
 static int batch_build(bssn_b200_batch *b) {
   std::vector<EvoDesc> descs(b->nevo);
-  std::vector<int> tile_evo;
+  long long ntiles = 0;
   std::vector<BatchOuterPt> layer[NGHOSTS], all_outer;
   std::vector<BatchInnerPt> inner;
   for (int e = 0; e < b->nevo; e++) {
@@ -146,15 +146,26 @@ static int batch_build(bssn_b200_batch *b) {
     d.tile_bz = k.bz;
     d.tiles_x = (n0 + k.bx - 1) / k.bx;
     d.tiles_y = (n1 + k.by - 1) / k.by;
-    d.tile_begin = (int)tile_evo.size();
     const long long nt = (long long)d.tiles_x * d.tiles_y * ((std::max(n2, 0) + k.bz - 1) / k.bz);
     b->padded_points += padded_points(n0, n1, std::max(n2, 0), k);
     b->interior_points += (long long)n0 * n1 * std::max(n2, 0);
-    if ((long long)tile_evo.size() + nt > (1LL << 30)) {
-      set_error("batch: too many tiles");
+    // chunks of up to kChunkEvos evolutions; a chunk's launch has one block per tile (x2 for
+    // 64-thread groups), which must stay below the grid limit
+    if (b->chunks.empty() || b->chunks.back().nevo == kChunkEvos) {
+      b->chunks.emplace_back();
+      memset(&b->chunks.back(), 0, sizeof(BatchChunk));
+    }
+    BatchChunk &c = b->chunks.back();
+    if ((long long)c.ntiles + nt > (1LL << 29)) {
+      set_error("batch: too many tiles in one chunk of evolutions");
       return BSSN_B200_EINVAL;
     }
-    tile_evo.insert(tile_evo.end(), (size_t)nt, e);
+    c.tile_begin[c.nevo] = c.ntiles;
+    c.evo[c.nevo] = d;
+    c.nevo++;
+    c.ntiles += (int)nt;
+    c.tile_begin[c.nevo] = c.ntiles;
+    ntiles += nt;
     // boundary lists (host copies of this evolution's bcstruct)
     const bc_info_struct &bi = G.bcstruct.bc_info;
     for (int gz = 0; gz < NGHOSTS; gz++)
@@ -181,9 +192,8 @@ static int batch_build(bssn_b200_batch *b) {
       for (const auto &q : h) inner.push_back(BatchInnerPt{e, q});
     }
   }
-  b->ntiles = (int)tile_evo.size();
+  b->ntiles = (int)std::min<long long>(ntiles, 1LL << 30);
   BSSN_TRY(upload(&b->d_descs, descs));
-  BSSN_TRY(upload(&b->d_tile_evo, tile_evo));
   for (int gz = 0; gz < NGHOSTS; gz++) {
     b->nouter_layer[gz] = (int)layer[gz].size();
     BSSN_TRY(upload(&b->d_outer_layer[gz], layer[gz]));
@@ -200,15 +210,15 @@ static int batch_build(bssn_b200_batch *b) {
 extern "C" {
 
 int bssn_b200_batch_create(int nevo, commondata_struct *const *cds, griddata_struct *const *gds, int tile_bx,
-                           int tile_by, int blocks, int steps_per_graph, void *stream, bssn_b200_batch **out) {
+                           int tile_by, int steps_per_graph, void *stream, bssn_b200_batch **out) {
   if (nevo < 1 || !cds || !gds || !out) {
     set_error("batch: need nevo >= 1 and non-NULL arrays");
     return BSSN_B200_EINVAL;
   }
   const bool per_grid = tile_bx == 0 && tile_by == 0;
-  if ((!per_grid && (tile_bx * tile_by != 128 || tile_bx < 1 || tile_by < 1)) || blocks < 1 || steps_per_graph < 1 ||
+  if ((!per_grid && (tile_bx * tile_by != 128 || tile_bx < 1 || tile_by < 1)) || steps_per_graph < 1 ||
       steps_per_graph > 1000) {
-    set_error("batch: tile %dx%d must have 128 points (or 0x0: a shape per evolution); blocks >= 1; "
+    set_error("batch: tile %dx%d must have 128 points (or 0x0: a shape per evolution); "
               "1 <= steps_per_graph <= 1000", tile_bx, tile_by);
     return BSSN_B200_EINVAL;
   }
@@ -222,7 +232,6 @@ int bssn_b200_batch_create(int nevo, commondata_struct *const *cds, griddata_str
   b->gds.assign(gds, gds + nevo);
   b->bx = tile_bx;
   b->by = tile_by;
-  b->blocks = blocks;
   b->steps_per_graph = steps_per_graph;
   b->stream = (cudaStream_t)stream;
   int rc = batch_build(b);

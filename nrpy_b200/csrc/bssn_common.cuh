@@ -187,7 +187,7 @@ struct EvoDesc {
   const double *xx0;
   int radial_sinh;  // 0: r = xx0 ; 1: SinhSpherical r(xx0)
   double AMPL, SINHW;
-  int tile_begin, tiles_x, tiles_y;  // this evolution's tiles in the batch tile list
+  int tiles_x, tiles_y;               // this evolution's tiles along i0 and i1
   int tile_bx, tile_by, tile_bz;     // its tile shape: tile_bx * tile_by * tile_bz = 128 points
 };
 struct BatchOuterPt {
@@ -206,12 +206,25 @@ __host__ __device__ inline void stage_io(const EvoDesc &d, int stage, double *&k
     default: kin = d.kodd; kout = d.y; break;
   }
 }
-// Batched launchers (pointwise.cu, boundary.cu): one launch covers every evolution.
-// `blocks` is the persistent grid size; each evolution's tile shape is in its EvoDesc.
-int launch_ricci_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                         cudaStream_t s);
-int launch_rhs_fused_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                             cudaStream_t s);
+// Up to kChunkEvos evolutions as one launch of a Ricci or RHS group kernel sees them. The
+// chunk is passed BY VALUE as the kernel parameter (it lands in the constant bank): every
+// block reads its evolution's descriptor there with a block-uniform index, so the fields the
+// point algebra uses throughout (strides, grid spacings, rfm and buffer pointers) stay
+// uniform operands instead of taking per-thread registers. With the descriptors in global
+// memory the same kernels spilled 300-600 bytes more per thread.
+constexpr int kChunkEvos = 120;
+struct BatchChunk {
+  int nevo;                         // evolutions in this chunk
+  int ntiles;                       // tiles of this chunk
+  int tile_begin[kChunkEvos + 1];   // first chunk-local tile of each evolution; [nevo] = ntiles
+  EvoDesc evo[kChunkEvos];
+};
+static_assert(sizeof(BatchChunk) + 16 <= 32764, "a BatchChunk must fit the 32764-byte kernel parameter space");
+// Batched launchers (pointwise.cu, boundary.cu). The Ricci and RHS group kernels run one
+// block per 128-point tile of a chunk; the boundary kernels cover every evolution in one
+// launch, reading the descriptor array in device memory.
+int launch_ricci_batched(Variant v, int stage, const BatchChunk &c, cudaStream_t s);
+int launch_rhs_fused_batched(Variant v, int stage, const BatchChunk &c, cudaStream_t s);
 int launch_radiation_batched(int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts, cudaStream_t s);
 int launch_rk_points_batched(Variant v, int stage, const EvoDesc *descs, const BatchOuterPt *pts, int npts,
                              cudaStream_t s);

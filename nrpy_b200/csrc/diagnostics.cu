@@ -70,11 +70,23 @@ Recipes default_recipes() {
   return r;
 }
 
-// Cartesian position and proper volume element of a cell (xx_to_Cart, sqrt_detgammahat_d3xx_volume_element).
+// Cartesian position and proper volume element of a cell (xx_to_Cart, sqrt_detgammahat_d3xx_volume_element),
+// with the expression trees of the generated functions so that coordinates agree to the last bit.
+enum CoordKind { KIND_SPHERICAL = 0, KIND_SINHSPHERICAL = 1, KIND_SINHCYLINDRICAL = 2 };
 struct CoordMap {
-  int sinh;
+  int kind;
   double AMPL, SINHW, ox, oy, oz, dxx0, dxx1, dxx2;
+  double AMPLRHO, SINHWRHO, AMPLZ, SINHWZ;
   __host__ __device__ void to_cart(double xx0, double xx1, double xx2, double out[3]) const {
+    if (kind == KIND_SINHCYLINDRICAL) {
+      const double t0 = 1.0 / SINHWRHO, t3 = 1.0 / SINHWZ;
+      const double rho = AMPLRHO * (exp(t0 * xx0) - exp(-t0 * xx0)) / (exp(t0) - exp(-t0));
+      out[0] = ox + rho * cos(xx1);
+      out[1] = oy + rho * sin(xx1);
+      out[2] = AMPLZ * (exp(t3 * xx2) - exp(-t3 * xx2)) / (exp(t3) - exp(-t3)) + oz;
+      return;
+    }
+    const int sinh = kind == KIND_SINHSPHERICAL;
     double rr;
     if (sinh) {
       const double t0 = 1.0 / SINHW;
@@ -87,10 +99,22 @@ struct CoordMap {
     out[1] = oy + t * sin(xx2);
     out[2] = oz + rr * cos(xx1);
   }
-  __device__ double dV(double xx0, double xx1) const {
-    const double s1 = sin(xx1);
+  __device__ double dV(double xx0, double xx1, double xx2) const {
     const double d3 = fabs(dxx0 * dxx1 * dxx2);
-    if (!sinh) return sqrt(xx0 * xx0 * xx0 * xx0 * (s1 * s1)) * d3;
+    if (kind == KIND_SINHCYLINDRICAL) {
+      // |rho'(xx0) rho(xx0) z'(xx2)| written as the generated square root of its square
+      const double t0 = 2.0 / SINHWRHO, t2 = 1.0 / SINHWZ;
+      const double t1 = exp(t0 * xx0);
+      const double a = 1.0 - t1, b = t1 + 1.0, e2 = exp(2.0 * t2 * xx2) + 1.0;
+      const double c0 = 1.0 - exp(t0), c2 = 1.0 - exp(2.0 * t2);
+      return AMPLRHO * AMPLRHO *
+             sqrt(a * a * (b * b) * (e2 * e2) *
+                  exp(t0 * t2 * (-SINHWRHO * xx2 + SINHWRHO - 2.0 * SINHWZ * xx0 + 2.0 * SINHWZ)) /
+                  (SINHWRHO * SINHWRHO * (SINHWZ * SINHWZ) * (c0 * c0 * c0 * c0) * (c2 * c2))) *
+             fabs(AMPLZ) * d3;
+    }
+    const double s1 = sin(xx1);
+    if (kind == KIND_SPHERICAL) return sqrt(xx0 * xx0 * xx0 * xx0 * (s1 * s1)) * d3;
     const double t0 = 1.0 / SINHW;
     const double t2 = exp(2.0 * t0 * xx0);
     const double a = 1.0 - t2, b = t2 + 1.0, c = 1.0 - exp(2.0 * t0);
@@ -101,12 +125,17 @@ struct CoordMap {
 };
 
 int coord_map(const params_struct *p, CoordMap *m) {
-  if (p->CoordSystem_hash != SPHERICAL && p->CoordSystem_hash != SINHSPHERICAL) {
+  int kind;
+  if (p->CoordSystem_hash == SPHERICAL) kind = KIND_SPHERICAL;
+  else if (p->CoordSystem_hash == SINHSPHERICAL) kind = KIND_SINHSPHERICAL;
+  else if (p->CoordSystem_hash == SINHCYLINDRICAL) kind = KIND_SINHCYLINDRICAL;
+  else {
     set_error("diagnostics: CoordSystem_hash %d not supported", p->CoordSystem_hash);
     return BSSN_B200_EINVAL;
   }
-  *m = CoordMap{p->CoordSystem_hash == SINHSPHERICAL, p->AMPL, p->SINHW, p->Cart_originx, p->Cart_originy,
-                p->Cart_originz, p->dxx0, p->dxx1, p->dxx2};
+  *m = CoordMap{kind,           p->AMPL,         p->SINHW,      p->Cart_originx, p->Cart_originy,
+                p->Cart_originz, p->dxx0,        p->dxx1,       p->dxx2,         p->AMPLRHO,
+                p->SINHWRHO,     p->AMPLZ,       p->SINHWZ};
   return BSSN_B200_OK;
 }
 
@@ -171,7 +200,7 @@ __global__ void integrate_kernel(const GridDims g, const CoordMap cm, const doub
     const long long r = t / n0;
     const int i1 = (int)(r % n1) + NGHOSTS, i2 = (int)(r / n1) + NGHOSTS;
     const double a0 = xx0[i0], a1 = xx1[i1], a2 = xx2[i2];
-    const double dV = cm.dV(a0, a1);
+    const double dV = cm.dV(a0, a1, a2);
     if (dV == 0.0) continue;
     double X[3];
     cm.to_cart(a0, a1, a2, X);
@@ -384,36 +413,68 @@ int nearest(const commondata_struct *cd, const griddata_struct *gd, const REAL *
     const int i1_mid = N1 / 2, i2_mid = N2 / 2;
     const int i1_max = N1 - NGHOSTS - 1;
     const int i2_q1 = (int)(NGHOSTS + 0.25 * (double)N2int - 0.5), i2_q3 = (int)(NGHOSTS + 0.75 * (double)N2int - 0.5);
+    const int i1_q1 = (int)(NGHOSTS + 0.25 * (double)N1int - 0.5), i1_q3 = (int)(NGHOSTS + 0.75 * (double)N1int - 0.5);
     auto cart = [&](int i0, int i1, int i2, double X[3]) { cm.to_cart(hx[0][i0], hx[1][i1], hx[2][i2], X); };
-    // sample lists in the reference's order (lines sorted by their coordinate)
+    // Sample lists in the reference's order (lines sorted by their coordinate). Spherical
+    // family: y lines at the equator and phi ~ +-pi/2, z lines at the two poles, the xy plane
+    // at the equator, the yz plane at phi ~ +-pi/2. Cylindrical family: y lines at phi ~ +-pi/2
+    // in the z mid-plane, the z line along the axis (innermost rho), the xy plane at mid z, the
+    // yz plane at phi ~ +-pi/2 (diagnostics_nearest_1d_y_and_z_axes.py:76-200,
+    // diagnostics_nearest_2d_xy_and_yz_planes.py:67-140).
     std::vector<Sample> ys, zs, xy, yz;
     double X[3];
-    for (int i2 : {i2_q1, i2_q3})
-      for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
-        cart(i0, i1_mid, i2, X);
-        ys.push_back({X[1], 0.0, IDX(i0, i1_mid, i2)});
+    const bool cylf = cm.kind == KIND_SINHCYLINDRICAL;
+    if (cylf) {
+      for (int i1 : {i1_q1, i1_q3})
+        for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
+          cart(i0, i1, i2_mid, X);
+          ys.push_back({X[1], 0.0, IDX(i0, i1, i2_mid)});
+        }
+      for (int i2 = NGHOSTS; i2 < N2 - NGHOSTS; i2++) {
+        cart(NGHOSTS, NGHOSTS, i2, X);
+        zs.push_back({X[2], 0.0, IDX(NGHOSTS, NGHOSTS, i2)});
       }
-    for (int i1 : {NGHOSTS, i1_max})
-      for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
-        cart(i0, i1, NGHOSTS, X);
-        zs.push_back({X[2], 0.0, IDX(i0, i1, NGHOSTS)});
-      }
+    } else {
+      for (int i2 : {i2_q1, i2_q3})
+        for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
+          cart(i0, i1_mid, i2, X);
+          ys.push_back({X[1], 0.0, IDX(i0, i1_mid, i2)});
+        }
+      for (int i1 : {NGHOSTS, i1_max})
+        for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
+          cart(i0, i1, NGHOSTS, X);
+          zs.push_back({X[2], 0.0, IDX(i0, i1, NGHOSTS)});
+        }
+    }
     auto by_coord = [](const Sample &a, const Sample &b) { return a.c0 < b.c0; };
     std::stable_sort(ys.begin(), ys.end(), by_coord);
     std::stable_sort(zs.begin(), zs.end(), by_coord);
-    for (int i2 = NGHOSTS; i2 < N2 - NGHOSTS; i2++)
-      for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
-        cart(i0, i1_mid, i2, X);
-        xy.push_back({X[0], X[1], IDX(i0, i1_mid, i2)});
-      }
-    for (int i2 : {i2_q1, i2_q3})
+    if (cylf) {
       for (int i1 = NGHOSTS; i1 < N1 - NGHOSTS; i1++)
         for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
-          cart(i0, i1, i2, X);
-          yz.push_back({X[1], X[2], IDX(i0, i1, i2)});
+          cart(i0, i1, i2_mid, X);
+          xy.push_back({X[0], X[1], IDX(i0, i1, i2_mid)});
         }
+      for (int i1 : {i1_q1, i1_q3})
+        for (int i2 = NGHOSTS; i2 < N2 - NGHOSTS; i2++)
+          for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
+            cart(i0, i1, i2, X);
+            yz.push_back({X[1], X[2], IDX(i0, i1, i2)});
+          }
+    } else {
+      for (int i2 = NGHOSTS; i2 < N2 - NGHOSTS; i2++)
+        for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
+          cart(i0, i1_mid, i2, X);
+          xy.push_back({X[0], X[1], IDX(i0, i1_mid, i2)});
+        }
+      for (int i2 : {i2_q1, i2_q3})
+        for (int i1 = NGHOSTS; i1 < N1 - NGHOSTS; i1++)
+          for (int i0 = NGHOSTS; i0 < N0 - NGHOSTS; i0++) {
+            cart(i0, i1, i2, X);
+            yz.push_back({X[1], X[2], IDX(i0, i1, i2)});
+          }
+    }
     (void)N0int;
-    (void)N1int;
     // one gather of every sample
     std::vector<int> idx;
     idx.push_back(IDX(NGHOSTS, i1_mid, i2_mid));

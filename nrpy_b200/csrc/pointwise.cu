@@ -560,11 +560,11 @@ int launch_rk_points(Variant v, int stage, double dt, const GridDims &g, const R
 }
 
 // ---------------------------------------------------------------- batched evolutions
-// Persistent kernels over a tile list that spans every evolution of a batch: block b takes
-// tiles b, b + gridDim.x, ... Tile t belongs to evolution tile_evo[t]; its local index runs
-// over (tiles_x, tiles_y, tiles_z) tiles of that evolution's shape tile_bx x tile_by x
-// tile_bz = 128 interior points (i0 fastest). A block has the group's NT threads (1-D) and
-// covers a tile in 128 / NT passes.
+// Ricci and fused RHS group kernels over a chunk of evolutions: block b takes tile
+// b / (128 / NT) of the chunk (a group with NT < 128 threads covers a tile in 128 / NT
+// blocks). The tile's evolution is found by a binary search over the chunk's tile_begin
+// table; its local index runs over (tiles_x, tiles_y, tiles_z) tiles of that evolution's
+// shape tile_bx x tile_by x tile_bz = 128 interior points (i0 fastest).
 __device__ __forceinline__ bool tile_point(const EvoDesc &d, int t_local, int lin, int &i0, int &i1, int &i2) {
   const int tx = t_local % d.tiles_x;
   const int r = t_local / d.tiles_x;
@@ -577,43 +577,47 @@ __device__ __forceinline__ bool tile_point(const EvoDesc &d, int t_local, int li
   return i0 < d.g.N0 - NGHOSTS && i1 < d.g.N1 - NGHOSTS && i2 < d.g.N2 - NGHOSTS;
 }
 
-template <Variant V, int G>
-__global__ void __launch_bounds__(RicciG<V, G>::NT, 1) ricci_batched_kernel(const EvoDesc *__restrict__ descs,
-                                                                          const int *__restrict__ tile_evo,
-                                                                          const int ntiles, const int stage) {
-  constexpr int NT = RicciG<V, G>::NT;
-  volatile double *sm = thread_slots<double>();
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const EvoDesc &d = descs[tile_evo[t]];
-    double *kin, *kout;
-    stage_io(d, stage, kin, kout);
-    for (int pass = 0; pass < (BX * BY) / NT; pass++) {
-      int i0, i1, i2;
-      if (!tile_point(d, t - d.tile_begin, pass * NT + threadIdx.x, i0, i1, i2)) continue;
-      ricci_body<V, G, double, NT>(d.g, d.rfm, kin, d.aux, i0, i1, i2, sm);
-    }
+// Evolution of chunk-local tile t: the last e with tile_begin[e] <= t.
+__device__ __forceinline__ int chunk_evo(const BatchChunk &c, int t) {
+  int lo = 0, hi = c.nevo;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (c.tile_begin[mid] <= t) lo = mid;
+    else hi = mid;
   }
+  return lo;
+}
+
+template <Variant V, int G>
+__global__ void __launch_bounds__(RicciG<V, G>::NT, 1) ricci_batched_kernel(const __grid_constant__ BatchChunk c,
+                                                                          const int stage) {
+  constexpr int NT = RicciG<V, G>::NT, PER = (BX * BY) / NT;
+  const int t = blockIdx.x / PER;
+  const int e = chunk_evo(c, t);
+  const EvoDesc &d = c.evo[e];
+  int i0, i1, i2;
+  if (!tile_point(d, t - c.tile_begin[e], (blockIdx.x % PER) * NT + threadIdx.x, i0, i1, i2)) return;
+  double *kin, *kout;
+  stage_io(d, stage, kin, kout);
+  volatile double *sm = thread_slots<double>();
+  ricci_body<V, G, double, NT>(d.g, d.rfm, kin, d.aux, i0, i1, i2, sm);
 }
 
 template <Variant V, int STAGE, int G>
-__global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_fused_batched_kernel(const EvoDesc *__restrict__ descs,
-                                                                            const int *__restrict__ tile_evo,
-                                                                            const int ntiles) {
-  constexpr int NT = RhsG<V, G>::NT;
-  // Plain slots: in the persistent batched kernels the RHS groups ran faster with them.
+__global__ void __launch_bounds__(RhsG<V, G>::NT, 1) rhs_fused_batched_kernel(const __grid_constant__ BatchChunk c) {
+  constexpr int NT = RhsG<V, G>::NT, PER = (BX * BY) / NT;
+  const int t = blockIdx.x / PER;
+  const int e = chunk_evo(c, t);
+  const EvoDesc &d = c.evo[e];
+  int i0, i1, i2;
+  if (!tile_point(d, t - c.tile_begin[e], (blockIdx.x % PER) * NT + threadIdx.x, i0, i1, i2)) return;
+  StageBuffers b;
+  b.y = d.y;
+  b.run = d.run;
+  stage_io(d, STAGE, b.kin, b.kout);
+  // Plain slots: the batched RHS groups ran faster with them.
   double *sm = const_cast<double *>(thread_slots<double>());
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const EvoDesc &d = descs[tile_evo[t]];
-    StageBuffers b;
-    b.y = d.y;
-    b.run = d.run;
-    stage_io(d, STAGE, b.kin, b.kout);
-    for (int pass = 0; pass < (BX * BY) / NT; pass++) {
-      int i0, i1, i2;
-      if (!tile_point(d, t - d.tile_begin, pass * NT + threadIdx.x, i0, i1, i2)) continue;
-      fused_body<V, double, STAGE, G, NT>(d.g, d.rfm, d.pp, d.aux, b, d.krhs, d.dt, i0, i1, i2, sm);
-    }
-  }
+  fused_body<V, double, STAGE, G, NT>(d.g, d.rfm, d.pp, d.aux, b, d.krhs, d.dt, i0, i1, i2, sm);
 }
 
 template <Variant V, int STAGE>
@@ -635,69 +639,59 @@ __global__ void rk_points_batched_kernel(const EvoDesc *__restrict__ descs, cons
 }
 
 template <Variant V, int G>
-static int launch_ricci_batched_group(int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                                      cudaStream_t s) {
+static int launch_ricci_batched_group(int stage, const BatchChunk &c, cudaStream_t s) {
   using Grp = RicciG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, double>();
   BSSN_TRY(set_smem(ricci_batched_kernel<V, G>, sb));
-  // `blocks` counts 128-thread CTAs; a group with fewer threads per CTA gets proportionally more.
-  ricci_batched_kernel<V, G><<<blocks * (BX * BY / Grp::NT), Grp::NT, sb, s>>>(descs, tile_evo, ntiles, stage);
+  ricci_batched_kernel<V, G><<<c.ntiles * (BX * BY / Grp::NT), Grp::NT, sb, s>>>(c, stage);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
 
 template <Variant V, int STAGE, int G>
-static int launch_fused_batched_group(const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                                      cudaStream_t s) {
+static int launch_fused_batched_group(const BatchChunk &c, cudaStream_t s) {
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, double>();
   BSSN_TRY(set_smem(rhs_fused_batched_kernel<V, STAGE, G>, sb));
-  rhs_fused_batched_kernel<V, STAGE, G><<<blocks * (BX * BY / Grp::NT), Grp::NT, sb, s>>>(descs, tile_evo, ntiles);
+  rhs_fused_batched_kernel<V, STAGE, G><<<c.ntiles * (BX * BY / Grp::NT), Grp::NT, sb, s>>>(c);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
 
 template <Variant V, int STAGE>
-static int launch_fused_batched_stage(const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                                      cudaStream_t s) {
-  return for_each_group<0, kRhsGroups>([&](auto gc) {
-    return launch_fused_batched_group<V, STAGE, decltype(gc)::value>(descs, tile_evo, ntiles, blocks, s);
-  });
+static int launch_fused_batched_stage(const BatchChunk &c, cudaStream_t s) {
+  return for_each_group<0, kRhsGroups>(
+      [&](auto gc) { return launch_fused_batched_group<V, STAGE, decltype(gc)::value>(c, s); });
 }
 
-int launch_ricci_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                         cudaStream_t s) {
-  if (ntiles <= 0) return BSSN_B200_OK;
+int launch_ricci_batched(Variant v, int stage, const BatchChunk &c, cudaStream_t s) {
+  if (c.ntiles <= 0) return BSSN_B200_OK;
   if (v != SPH_3D && v != SINH_3D) {
     set_error("batched evolutions: only full 3-D variants are instantiated");
     return BSSN_B200_EINVAL;
   }
   if (v == SPH_3D) {
-    return for_each_group<0, kRicciGroups>([&](auto gc) {
-      return launch_ricci_batched_group<SPH_3D, decltype(gc)::value>(stage, descs, tile_evo, ntiles, blocks, s);
-    });
+    return for_each_group<0, kRicciGroups>(
+        [&](auto gc) { return launch_ricci_batched_group<SPH_3D, decltype(gc)::value>(stage, c, s); });
   }
-  return for_each_group<0, kRicciGroups>([&](auto gc) {
-    return launch_ricci_batched_group<SINH_3D, decltype(gc)::value>(stage, descs, tile_evo, ntiles, blocks, s);
-  });
+  return for_each_group<0, kRicciGroups>(
+      [&](auto gc) { return launch_ricci_batched_group<SINH_3D, decltype(gc)::value>(stage, c, s); });
 }
 
 template <Variant V>
-static int launch_fused_batched_v(int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                                  cudaStream_t s) {
+static int launch_fused_batched_v(int stage, const BatchChunk &c, cudaStream_t s) {
   switch (stage) {
-    case 1: return launch_fused_batched_stage<V, 1>(descs, tile_evo, ntiles, blocks, s);
-    case 2: return launch_fused_batched_stage<V, 2>(descs, tile_evo, ntiles, blocks, s);
-    case 3: return launch_fused_batched_stage<V, 3>(descs, tile_evo, ntiles, blocks, s);
-    default: return launch_fused_batched_stage<V, 4>(descs, tile_evo, ntiles, blocks, s);
+    case 1: return launch_fused_batched_stage<V, 1>(c, s);
+    case 2: return launch_fused_batched_stage<V, 2>(c, s);
+    case 3: return launch_fused_batched_stage<V, 3>(c, s);
+    default: return launch_fused_batched_stage<V, 4>(c, s);
   }
 }
 
-int launch_rhs_fused_batched(Variant v, int stage, const EvoDesc *descs, const int *tile_evo, int ntiles, int blocks,
-                             cudaStream_t s) {
-  if (ntiles <= 0) return BSSN_B200_OK;
-  if (v == SPH_3D) return launch_fused_batched_v<SPH_3D>(stage, descs, tile_evo, ntiles, blocks, s);
-  if (v == SINH_3D) return launch_fused_batched_v<SINH_3D>(stage, descs, tile_evo, ntiles, blocks, s);
+int launch_rhs_fused_batched(Variant v, int stage, const BatchChunk &c, cudaStream_t s) {
+  if (c.ntiles <= 0) return BSSN_B200_OK;
+  if (v == SPH_3D) return launch_fused_batched_v<SPH_3D>(stage, c, s);
+  if (v == SINH_3D) return launch_fused_batched_v<SINH_3D>(stage, c, s);
   set_error("batched evolutions: only full 3-D variants are instantiated");
   return BSSN_B200_EINVAL;
 }

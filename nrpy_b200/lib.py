@@ -208,8 +208,8 @@ SIGNATURES = [
     ("bssn_b200_kernel_launches", C.c_ulonglong, []),
     ("bssn_b200_rhs_fused_stage", C.c_int, [PCD, PGD, C.c_int, C.c_int, V]),
     ("bssn_b200_fp64_fma_rate", C.c_int, [C.c_int, C.POINTER(C.c_double), V]),
-    ("bssn_b200_batch_create", C.c_int, [C.c_int, C.POINTER(PCD), C.POINTER(PGD), C.c_int, C.c_int, C.c_int,
-                                         C.c_int, V, C.POINTER(V)]),
+    ("bssn_b200_batch_create", C.c_int, [C.c_int, C.POINTER(PCD), C.POINTER(PGD), C.c_int, C.c_int, C.c_int, V,
+                                         C.POINTER(V)]),
     ("bssn_b200_batch_run", C.c_int, [V, C.c_int]),
     ("bssn_b200_batch_info", C.c_int, [V, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
                                        C.POINTER(C.c_ulonglong)]),

@@ -16,12 +16,13 @@ import pytest
 import torch
 
 from oracle import ref as oref
-from tests.util import rel_l2_per_gf
+from tests.util import compare_diagnostics_dirs, rel_l2_per_gf
 
 from tests.sinhaxi_cases import test_sinhaxi_20_steps, test_sinhaxi_ricci_rhs  # noqa: F401  (oracle sinhaxi8)
 from tests.sinhcyl_cases import (  # noqa: F401  (SinhCylindrical at 8th order: oracle variant sinhcyl8)
     test_sinhcyl_20_steps,
     test_sinhcyl_brill_lindquist_50_steps,
+    test_sinhcyl_diagnostics_files,
     test_sinhcyl_grid_bcstruct_and_initial_data,
     test_sinhcyl_ricci_rhs_constraints,
 )
@@ -198,7 +199,7 @@ def test_batch_equals_single_grid_path(cuda):
              dict(coord="Spherical", Nxx=(37, 12, 4), grid_physical_size=7.5, BH1_mass=0.31, BH1_posn_z=0.7,
                   BH2_mass=0.66, BH2_posn_z=-0.7)]
     be = BatchedEvolutions(specs)
-    be.build(tile=(32, 4), blocks=148, steps_per_graph=2)
+    be.build(tile=(32, 4), steps_per_graph=2)
     be.run(2)
     torch.cuda.synchronize()
     for spec, g in zip(specs, be.grids):
@@ -211,13 +212,6 @@ def test_batch_equals_single_grid_path(cuda):
         assert np.nanmax(np.where(np.linalg.norm(a, axis=1) > 0, err, 0)) <= 1e-14, err
         single.close()
     be.close()
-
-
-def _read(path):
-    comments, rows = [], []
-    for line in path.read_text().splitlines():
-        (comments if line.startswith("#") else rows).append(line)
-    return comments, np.array([[float(x) for x in r.split()] for r in rows])
 
 
 def test_diagnostics_files_match_reference(cuda, tmp_path, monkeypatch):
@@ -236,19 +230,7 @@ def test_diagnostics_files_match_reference(cuda, tmp_path, monkeypatch):
     g.diagnostics(0.25, nn=0, time=0.0)
     torch.cuda.synchronize()
     monkeypatch.chdir(tmp_path)
-    names = sorted(p.name for p in (tmp_path / "ref").iterdir())
-    assert names and sorted(p.name for p in (tmp_path / "ours").iterdir()) == names
-    for name in names:
-        c_ref, d_ref = _read(tmp_path / "ref" / name)
-        c_ours, d_ours = _read(tmp_path / "ours" / name)
-        assert c_ours == c_ref and d_ours.shape == d_ref.shape, name
-        if name.startswith("out3d"):
-            np.testing.assert_allclose(d_ours, d_ref, rtol=1e-10, atol=0, err_msg=name)
-            continue
-        nc = 1 if name.startswith(("out0d", "out1d")) else 2
-        np.testing.assert_allclose(d_ours[:, :nc], d_ref[:, :nc], rtol=1e-12, atol=1e-12, err_msg=name)
-        scale = np.abs(d_ref[:, nc:]).max(axis=0)
-        assert np.all(np.abs(d_ours[:, nc:] - d_ref[:, nc:]) <= 1e-9 * scale + 1e-300), name
+    compare_diagnostics_dirs(tmp_path / "ref", tmp_path / "ours")
     rg.close()
     g.close()
 

@@ -7,7 +7,7 @@ order, in the child process). Bars as for the Spherical family: bit-exact grid, 
 bcstruct; initial data alpha and W to 1e-13 relative on the interior and every value to 1e-11;
 Ricci and the RHS to 1e-12 per-gridfunction relative L2 (the RHS of trK to 1e-11, see the
 test); 20 RK4 steps to 1e-10 (both stage orders, radiation and extrapolation outer BCs); the
-constraint integrals to 1e-10.
+constraint integrals to 1e-10; the diagnostics() files with the bars of the spherical families.
 """
 
 import numpy as np
@@ -15,7 +15,7 @@ import pytest
 import torch
 
 from oracle import ref as oref
-from tests.util import rel_l2_per_gf
+from tests.util import compare_diagnostics_dirs, rel_l2_per_gf
 
 pytestmark = pytest.mark.gpu
 
@@ -158,5 +158,30 @@ def test_sinhcyl_brill_lindquist_50_steps(cuda):
     den = np.sqrt((r**2).sum(axis=1))
     err = num / np.where(den < 1e-8 * den.max(), den.max(), den)  # vanishing phi components: against the largest
     assert err.max() <= 1e-10, err
+    rg.close()
+    g.close()
+
+
+def test_sinhcyl_diagnostics_files(cuda, tmp_path, monkeypatch):
+    """diagnostics() of a perturbed state at two output steps against the reference's own:
+    the grid-centre point, the y lines at phi = +-pi/2 in the z mid-plane, the z line along the
+    axis, the xy plane at mid z, the yz plane at phi = +-pi/2, and the volume integrals with the
+    SinhCylindrical volume element."""
+    rg, g, ng = _pair()
+    state = oref.perturbed_state(rg, seed=4)
+    rg.set_y_n(state)
+    g.y_n.copy_(torch.from_numpy(state).to(g.device))
+    for d in ("ref", "ours"):
+        (tmp_path / d).mkdir()
+    for nn, t in [(0, 0.0), (7, 0.25)]:
+        monkeypatch.chdir(tmp_path / "ref")
+        rg.diagnostics(nn, t, 0.25)
+        monkeypatch.chdir(tmp_path / "ours")
+        g.diagnostics(0.25, nn=nn, time=t)
+        torch.cuda.synchronize()
+    monkeypatch.chdir(tmp_path)
+    names = compare_diagnostics_dirs(tmp_path / "ref", tmp_path / "ours")
+    assert any(n.startswith("out1d-z-SinhCylindrical") for n in names)
+    assert any("sphere_R_gt_8" in n for n in names)
     rg.close()
     g.close()

@@ -25,7 +25,7 @@ def test_batch_equals_single_grid_path(cuda, tile):
     from nrpy_b200.grid import BSSNGrid
 
     be = BatchedEvolutions(SPECS)
-    be.build(tile=tile, blocks=148, steps_per_graph=2)
+    be.build(tile=tile, steps_per_graph=2)
     be.run(3)  # 6 RK4 steps
     torch.cuda.synchronize()
     for spec, g in zip(SPECS, be.grids):
@@ -58,7 +58,7 @@ def test_batch_matches_reference_oracle(cuda):
         g.y_n.copy_(torch.from_numpy(inp).to(g.device))
         rg.step(10)
         refs.append(rg)
-    be.build(tile=(32, 4), blocks=296, steps_per_graph=5)
+    be.build(tile=(32, 4), steps_per_graph=5)
     be.run(2)
     torch.cuda.synchronize()
     for rg, g in zip(refs, be.grids):
@@ -73,8 +73,35 @@ def test_autotuner_picks_a_measured_configuration(cuda):
 
     be = BatchedEvolutions(SPECS)
     y0 = [g.y_n.clone() for g in be.grids]
-    res = be.autotune(steps=1, tiles=[(32, 4), (64, 2)], blocks_per_sm=(1, 2))
-    assert len(res["table"]) == 4 and res["ms_per_step"] == min(r["ms_per_step"] for r in res["table"])
+    res = be.autotune(steps=1, tiles=[(32, 4), (64, 2)])
+    assert len(res["table"]) == 2 and res["ms_per_step"] == min(r["ms_per_step"] for r in res["table"])
     for g, y in zip(be.grids, y0):
         assert torch.equal(g.y_n, y)  # states restored
+    be.close()
+
+
+def test_batch_of_more_evolutions_than_one_launch_holds(cuda):
+    """125 small evolutions: more than the 120 descriptors one launch of a group kernel carries,
+    so every stage runs two launches per group kernel. Evolutions on both sides of the split
+    must equal the single-grid path after 4 RK4 steps."""
+    from nrpy_b200.batch import BatchedEvolutions
+    from nrpy_b200.grid import BSSNGrid
+
+    rng = np.random.default_rng(11)
+    specs = [dict(coord="Spherical", Nxx=(int(rng.integers(8, 20)), int(rng.integers(4, 9)), 2 * int(rng.integers(1, 3))),
+                  grid_physical_size=7.5, BH1_mass=float(rng.uniform(0.3, 0.7)), BH1_posn_z=0.4,
+                  BH2_mass=float(rng.uniform(0.3, 0.7)), BH2_posn_z=-0.4) for _ in range(125)]
+    be = BatchedEvolutions(specs)
+    be.build(tile=(0, 0), steps_per_graph=2)
+    be.run(2)
+    torch.cuda.synchronize()
+    for k in (0, 119, 120, 124):
+        single = BSSNGrid(**specs[k])
+        single.MoL_step_forward_in_time(mode=1, nsteps=4)
+        torch.cuda.synchronize()
+        a = single.y_n.view(24, -1).cpu().numpy()
+        b = be.grids[k].y_n.view(24, -1).cpu().numpy()
+        err = rel_l2_per_gf(b, a, floor=1e-300)
+        assert np.nanmax(np.where(np.linalg.norm(a, axis=1) > 0, err, 0)) <= 1e-14, (k, err)
+        single.close()
     be.close()

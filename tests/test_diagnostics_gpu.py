@@ -8,21 +8,13 @@ output steps. The file names and every comment line must be identical; numbers a
 H and M^2, and 1e-10 relative for the integrals.
 """
 
-import pathlib
-
-import numpy as np
 import pytest
+
+from tests.util import compare_diagnostics_dirs
 
 pytestmark = pytest.mark.gpu
 
 CASES = [("sph3d", "Spherical", (24, 8, 8), 7.5), ("sinh3d", "SinhSpherical", (24, 8, 8), 10.0)]
-
-
-def read(path: pathlib.Path):
-    comments, rows = [], []
-    for line in path.read_text().splitlines():
-        (comments if line.startswith("#") else rows).append(line)
-    return comments, np.array([[float(x) for x in r.split()] for r in rows])
 
 
 @pytest.mark.parametrize("variant,coord,nxx,gps", CASES)
@@ -51,20 +43,5 @@ def test_diagnostics_files_match_reference(cuda, tmp_path, monkeypatch, variant,
         torch.cuda.synchronize()
     rg.close()
     monkeypatch.chdir(tmp_path)
-    names_ref = sorted(p.name for p in (tmp_path / "ref").iterdir())
-    names_ours = sorted(p.name for p in (tmp_path / "ours").iterdir())
-    assert names_ours == names_ref
-    assert any(n.startswith("out0d") for n in names_ref) and any(n.startswith("out3d") for n in names_ref)
-    for name in names_ref:
-        c_ref, d_ref = read(tmp_path / "ref" / name)
-        c_ours, d_ours = read(tmp_path / "ours" / name)
-        assert c_ours == c_ref, name
-        assert d_ours.shape == d_ref.shape, name
-        if name.startswith("out3d"):
-            np.testing.assert_allclose(d_ours, d_ref, rtol=1e-10, atol=0, err_msg=name)
-            continue
-        ncoord = 1 if name.startswith(("out0d", "out1d")) else 2
-        np.testing.assert_allclose(d_ours[:, :ncoord], d_ref[:, :ncoord], rtol=1e-12, atol=1e-12, err_msg=name)
-        vals_ref, vals_ours = d_ref[:, ncoord:], d_ours[:, ncoord:]
-        scale = np.abs(vals_ref).max(axis=0)
-        assert np.all(np.abs(vals_ours - vals_ref) <= 1e-9 * scale + 1e-300), name
+    names = compare_diagnostics_dirs(tmp_path / "ref", tmp_path / "ours")
+    assert any(n.startswith("out0d") for n in names) and any(n.startswith("out3d") for n in names)

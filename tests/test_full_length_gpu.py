@@ -156,7 +156,7 @@ def test_batch_64_evolutions_100_steps_against_reference(cuda):
     specs = batching_workload(seed=7, n=64)
     be = BatchedEvolutions(specs)
     y0 = [g.y_n.cpu().numpy() for g in be.grids]
-    be.build(tile=(0, 0), blocks=296, steps_per_graph=20)  # a tile shape per grid
+    be.build(tile=(0, 0), steps_per_graph=20)  # a tile shape per grid
     be.run(5)  # 100 RK4 steps
     torch.cuda.synchronize()
     worst, compared, nonfinite = 0.0, 0, []

@@ -45,3 +45,32 @@ def smooth_fields(xx, seed: int, amp: float = 0.05, ngfs: int = 24) -> np.ndarra
         a = amp * rng.uniform(0.5, 1.0)
         out[gf] = a * np.sin(k0 * np.pi * X0 / x0max + p0) * np.cos(k1 * X1 + p1) * np.cos(k2 * X2 + p2)
     return out
+
+
+def read_diagnostics_file(path: pathlib.Path):
+    """Comment lines and the numeric rows of one diagnostics output file."""
+    comments, rows = [], []
+    for line in path.read_text().splitlines():
+        (comments if line.startswith("#") else rows).append(line)
+    return comments, np.array([[float(x) for x in r.split()] for r in rows])
+
+
+def compare_diagnostics_dirs(ref_dir: pathlib.Path, ours_dir: pathlib.Path) -> list:
+    """The diagnostics() files of two runs: the same names and identical comment lines;
+    coordinates to 1e-12, sampled values to 1e-9 of each column's largest magnitude, volume
+    integrals (out3d) to 1e-10 relative. Returns the compared names."""
+    names = sorted(p.name for p in ref_dir.iterdir())
+    assert names and sorted(p.name for p in ours_dir.iterdir()) == names
+    for name in names:
+        c_ref, d_ref = read_diagnostics_file(ref_dir / name)
+        c_ours, d_ours = read_diagnostics_file(ours_dir / name)
+        assert c_ours == c_ref, name
+        assert d_ours.shape == d_ref.shape, name
+        if name.startswith("out3d"):
+            np.testing.assert_allclose(d_ours, d_ref, rtol=1e-10, atol=0, err_msg=name)
+            continue
+        nc = 1 if name.startswith(("out0d", "out1d")) else 2
+        np.testing.assert_allclose(d_ours[:, :nc], d_ref[:, :nc], rtol=1e-12, atol=1e-12, err_msg=name)
+        scale = np.abs(d_ref[:, nc:]).max(axis=0)
+        assert np.all(np.abs(d_ours[:, nc:] - d_ref[:, nc:]) <= 1e-9 * scale + 1e-300), name
+    return names
