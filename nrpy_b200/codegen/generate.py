@@ -61,6 +61,13 @@ RHS_ALLOC = [(True, False, "dfs"), (True, False, "sched")]
 # stencil loads) even with a few local-memory spills.
 RICCI_CAPS = [160, 150]
 RHS_CAPS = [72, 80]
+# The FP32 (mixed-precision) instantiations get their own allocation where a budget of their
+# own was faster: an FP32 value takes one register instead of two. Timed on SinhSpherical
+# 256x64x32 with the FP32 algebra (tune_groups generate-caps --dtype float, budgets 72 to 250):
+# Ricci group 0 87.6 -> 71.8 us and group 1 81.6 -> 65.8 us with every value in registers
+# (budget 250); RHS group 1 171 -> 160 us at budget 200; RHS group 0 was fastest at 72.
+RICCI_CAPS_F32 = [250, 250]
+RHS_CAPS_F32 = [72, 200]
 # Value types for which a group's slot array is plain instead of volatile (volatile: every slot
 # access stays where the allocator put it; plain: the compiler may schedule the accesses), per
 # group, from a timing sweep: plain slots help the RHS groups in FP32 and cost in FP64.
@@ -88,25 +95,37 @@ ADJ_REG_CAPACITY = 150
 ADJ_REMAT = dict(remat_first=True, deriv_remat=True, order="sched_dfs")
 
 
-def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int, plain_slots=()) -> str:
+def _group_struct(kind: str, tag: str, g: int, fname: str, gfs, slots: int, plain_slots=(),
+                  fname_f32: str = "", slots_f32: int = -1) -> str:
+    """The group's descriptor struct. With fname_f32, FP32 evaluations (T = float) call that
+    function, which has an allocation of its own with slots_f32 slots."""
     cases = " ".join(f"case {k}: return {x};" for k, x in enumerate(gfs))
     # The kernels hand a group a volatile slot pointer, or a plain one to ask for plain slots;
     # for the value types listed in plain_slots the group drops the qualifier itself (the
     # dynamic shared memory is not a volatile object).
     plain = " || ".join(["!std::is_volatile<S>::value"] + [f"std::is_same<T, {t}>::value" for t in plain_slots])
+    if not fname_f32:
+        fname_f32, slots_f32 = fname, slots
+    nt = threads_for(slots)
+    assert 2 * slots_f32 * 4 * nt <= SMEM_PER_SM, "FP32 slots must fit the FP64 block size"
+
+    def call(sm: str) -> str:
+        return (f"if constexpr (std::is_same<T, float>::value) {fname_f32}<T, TF, NTB>(ctx, out, {sm});\n"
+                f"      else {fname}<T, TF, NTB>(ctx, out, {sm});")
     return (
         f"template <> struct {kind}_{tag}<{g}> {{\n"
         f"  static constexpr int N = {len(gfs)};\n"
-        f"  static constexpr int SLOTS = {slots};\n"
-        f"  static constexpr int NT = {threads_for(slots)};  // threads per block of the single-grid kernels\n"
+        f"  static constexpr int SLOTS = {slots};          // per-thread slots of the FP64 evaluation\n"
+        f"  static constexpr int SLOTS_F32 = {slots_f32};  // and of the FP32 evaluation\n"
+        f"  static constexpr int NT = {nt};  // threads per block of the single-grid kernels\n"
         f"  __host__ __device__ static constexpr int GF(int k) {{\n"
         f"    switch (k) {{ {cases} }}\n    return -1;\n  }}\n"
         f"  template <typename T, typename TF, int NTB, typename Ctx, typename S>\n"
         f"  __device__ __forceinline__ static void eval(const Ctx &ctx, T *out, S *sm) {{\n"
         f"    if constexpr ({plain}) {{\n"
-        f"      {fname}<T, TF, NTB>(ctx, out, const_cast<T *>(sm));\n"
+        f"      {call('const_cast<T *>(sm)')}\n"
         f"    }} else {{\n"
-        f"      {fname}<T, TF, NTB>(ctx, out, sm);\n"
+        f"      {call('sm')}\n"
         f"    }}\n  }}\n}};\n"
     )
 
@@ -143,8 +162,18 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
         )
         parts.append(code)
         stats[f"ricci_g{g}"] = st
+        f32 = {}
+        if RICCI_CAPS_F32[g] != cap:
+            code, st32 = emit_point_function(
+                fname + "_f32", [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
+                comment=f"Rbar_ij {names}, {coord}: the FP32 evaluation's allocation",
+                reg_capacity=RICCI_CAPS_F32[g], remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+            )
+            parts.append(code)
+            stats[f"ricci_g{g}_f32"] = st32
+            f32 = dict(fname_f32=fname + "_f32", slots_f32=st32["smem_slots"])
         structs.append(_group_struct("RicciGroup", tag, g, fname, [be.RBAR_ORDER.index(k) for k in names],
-                                     st["smem_slots"], RICCI_PLAIN_SLOTS[g]))
+                                     st["smem_slots"], RICCI_PLAIN_SLOTS[g], **f32))
     for g, names in enumerate(RHS_GROUPS):
         fname = f"rhs_point_{tag}_g{g}"
         remat_first, deriv_remat, order = RHS_ALLOC[g]
@@ -156,8 +185,18 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
         )
         parts.append(code)
         stats[f"rhs_g{g}"] = st
+        f32 = {}
+        if RHS_CAPS_F32[g] != cap:
+            code, st32 = emit_point_function(
+                fname + "_f32", [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU,
+                symmetry_axes=sym, comment=f"BSSN RHS + KO (CAKO) of {names}, {coord}: the FP32 evaluation's allocation",
+                reg_capacity=RHS_CAPS_F32[g], remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+            )
+            parts.append(code)
+            stats[f"rhs_g{g}_f32"] = st32
+            f32 = dict(fname_f32=fname + "_f32", slots_f32=st32["smem_slots"])
         structs.append(_group_struct("RhsGroup", tag, g, fname, [be.GF_ORDER.index(k) for k in names],
-                                     st["smem_slots"], RHS_PLAIN_SLOTS[g]))
+                                     st["smem_slots"], RHS_PLAIN_SLOTS[g], **f32))
     code, st = emit_point_function(
         f"constraints_point_{tag}",
         [(f"out[{i}]", cons[k]) for i, k in enumerate(["H", "MSQUARED", "LAMBDA_CONSTRAINT"])],
@@ -190,7 +229,8 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
     hdr = (
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', {fd_order}th-order FD, KO (CAKO).\n"
-        f"// Register budgets Ricci {RICCI_CAPS}, RHS {RHS_CAPS} values; allocation (remat_first, deriv_remat, "
+        f"// Register budgets Ricci {RICCI_CAPS}, RHS {RHS_CAPS} values (FP32 evaluation: Ricci {RICCI_CAPS_F32}, "
+        f"RHS {RHS_CAPS_F32}); allocation (remat_first, deriv_remat, "
         f"order): Ricci {RICCI_ALLOC}, RHS {RHS_ALLOC}; plain slots Ricci {RICCI_PLAIN_SLOTS}, RHS {RHS_PLAIN_SLOTS}.\n"
         f"// Per point: {stats}\n"
         "#pragma once\n\n"

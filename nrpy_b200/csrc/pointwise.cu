@@ -82,8 +82,9 @@ struct RegCtx {
 #undef invdxx2
 
 // Output-group traits of the generated variants: RicciGroup<V,G> / RhsGroup<V,G> expose
-// N (outputs), GF[] (their gridfunction indices), SLOTS (per-thread shared-memory slots of
-// the spilled values) and eval().
+// N (outputs), GF[] (their gridfunction indices), SLOTS / SLOTS_F32 (per-thread shared-memory
+// slots of the spilled values in the FP64 and in the FP32 evaluation, which may have
+// allocations of their own) and eval().
 template <Variant V, int G>
 using RicciG = std::conditional_t<
     V == SPH_3D, RicciGroup_sph_3d<G>,
@@ -403,7 +404,7 @@ static bool empty_interior(const GridDims &g) {
 // Dynamic shared memory of a group kernel: SLOTS values of type T for each of its NT threads.
 template <typename Grp, typename T>
 constexpr size_t slot_bytes() {
-  return (size_t)Grp::SLOTS * Grp::NT * sizeof(T);
+  return (size_t)(std::is_same<T, float>::value ? Grp::SLOTS_F32 : Grp::SLOTS) * Grp::NT * sizeof(T);
 }
 
 template <typename KernelPtr>
