@@ -225,11 +225,13 @@ def generate_orders() -> None:
         print(tag, flush=True)
 
 
-def generate_caps(caps, fd_order: int = 4, dtype: str = "double") -> None:
+def generate_caps(caps, fd_order: int = 4, dtype: str = "double", groups=None) -> None:
     """The present groups with their chosen allocation and order (generate.py) at several
     register budgets, at the given finite-difference order, evaluated in `dtype` (double, or
     float as the mixed-precision kernels run them: FP32 algebra on FP64 finite differences,
-    with the slot qualifier generate.py gives FP32 groups)."""
+    with the slot qualifier generate.py gives FP32 groups). `groups` names other candidate
+    groups (CANDIDATES) to time instead of the present ones; they get the allocation of the
+    present first group of their kind."""
     from nrpy_b200.codegen import bssn_exprs as be
     from nrpy_b200.codegen import fdcoeffs as fdc
     from nrpy_b200.codegen.emit_cuda import emit_point_function
@@ -242,8 +244,12 @@ def generate_caps(caps, fd_order: int = 4, dtype: str = "double") -> None:
     OUT.mkdir(parents=True, exist_ok=True)
     chosen = dict(zip(ORDER_GROUPS, list(RICCI_ALLOC) + list(RHS_ALLOC)))
     plain = dict(zip(ORDER_GROUPS, [dtype in t for t in list(RICCI_PLAIN_SLOTS) + list(RHS_PLAIN_SLOTS)]))
+    for gname in groups or []:
+        kind = CANDIDATES[gname][0]
+        chosen.setdefault(gname, RICCI_ALLOC[0] if kind == "ricci" else RHS_ALLOC[0])
+        plain.setdefault(gname, dtype in (RICCI_PLAIN_SLOTS[0] if kind == "ricci" else RHS_PLAIN_SLOTS[0]))
     vbytes = 4 if dtype == "float" else 8
-    for gname in ORDER_GROUPS:
+    for gname in groups or ORDER_GROUPS:
         kind, names = CANDIDATES[gname]
         src, uv = (ricci, None) if kind == "ricci" else (rhs, betaU)
         rf, dr, order = chosen[gname]
@@ -379,6 +385,7 @@ if __name__ == "__main__":
     ap.add_argument("--caps", default="72,80,90,100")
     ap.add_argument("--fd-order", type=int, default=4)
     ap.add_argument("--dtype", default="double", choices=["double", "float"], help="value type of generate-caps")
+    ap.add_argument("--groups", default="", help="generate-caps: candidate groups to time (default: the present ones)")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--log", default=None)
     a = ap.parse_args()
@@ -387,7 +394,7 @@ if __name__ == "__main__":
     elif a.step == "generate-orders":
         generate_orders()
     elif a.step == "generate-caps":
-        generate_caps([int(c) for c in a.caps.split(",")], a.fd_order, a.dtype)
+        generate_caps([int(c) for c in a.caps.split(",")], a.fd_order, a.dtype, [g for g in a.groups.split(",") if g])
     elif a.step == "generate-leaf":
         generate_leaf()
     elif a.step == "compile":
