@@ -7,6 +7,7 @@ flags in generate.py come from its measurements). Three steps:
   python -m nrpy_b200.codegen.tune_groups generate-orders  # present groups x statement orders
   python -m nrpy_b200.codegen.tune_groups generate-caps    # present groups x register budgets
   python -m nrpy_b200.codegen.tune_groups generate-leaf    # present groups on precomputed FD leaves
+  python -m nrpy_b200.codegen.tune_groups generate-staged  # Ricci groups on shared-memory tiles
   python -m nrpy_b200.codegen.tune_groups compile    # nvcc, sm_100a, no GPU needed
   python -m nrpy_b200.codegen.tune_groups run        # on a B200; prints one line per kernel
 
@@ -342,6 +343,194 @@ def generate_leaf() -> None:
     print(f"leaf: {n} leaves", flush=True)
 
 
+STAGED_HARNESS = r'''// Feasibility: Ricci group kernels reading their 9 stencil gridfunctions (hDD, lambdaU) from a
+// shared-memory copy of the tile plus a 2-point halo, against the same groups reading global memory.
+#define TUNE_NG 3
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
+#include <cuda_runtime.h>
+struct RfmArrays { const double *f0, *f0_D0, *f0_DD00, *f0_DDD000, *f1, *f1_D1, *f1_DD11; };
+template <typename T> __device__ __forceinline__ T ipow(T x, int n) { T r = x; for (int k = 1; k < n; k++) r *= x; return r; }
+struct PointCtx {
+  const double *__restrict__ in; const double *__restrict__ aux; int s1, s2, ntot; int i0, i1;
+  double invdxx0, invdxx1, invdxx2; RfmArrays rfm;
+  __device__ __forceinline__ double ld(int gf, int a, int b, int c) const { return __ldg(in + (gf * ntot + (a + b * s1 + c * s2))); }
+};
+template <int SX, int SY, int SZ>
+struct SmemCtx {
+  const double *s;  // this thread's centre in the staged box of gridfunction 11
+  int i0, i1;
+  double invdxx0, invdxx1, invdxx2; RfmArrays rfm;
+  __device__ __forceinline__ double ld(int gf, int a, int b, int c) const {
+    return s[(gf - 11) * (SX * SY * SZ) + c * (SX * SY) + b * SX + a];
+  }
+};
+#define LD(gf, a, b, c) ctx.ld(gf, a, b, c)
+#define RFM(arr, d) __ldg(ctx.rfm.arr + ctx.i##d)
+#define rfm_f0 f0
+#define rfm_f0_D0 f0_D0
+#define rfm_f0_DD00 f0_DD00
+#define rfm_f0_DDD000 f0_DDD000
+#define rfm_f1 f1
+#define rfm_f1_D1 f1_D1
+#define rfm_f1_DD11 f1_DD11
+#define PARAM(name) ctx.name
+#define SMEM(k) sm[(k) * NT]
+#define invdxx0 ctx.invdxx0
+#define invdxx1 ctx.invdxx1
+#define invdxx2 ctx.invdxx2
+#include "staged_ricci.cuh"
+#undef invdxx0
+#undef invdxx1
+#undef invdxx2
+constexpr int NG = TUNE_NG, N0 = 256 + 2 * NG, N1 = 64 + 2 * NG, N2 = 32 + 2 * NG, NTOT = N0 * N1 * N2;
+struct G0 { template <int NT, class C, class S> __device__ __forceinline__ static void eval(const C &c, double *o, S *sm) { @G0FN@<double, double, NT>(c, o, sm); } static constexpr int SLOTS = @G0SLOTS@; };
+struct G1 { template <int NT, class C, class S> __device__ __forceinline__ static void eval(const C &c, double *o, S *sm) { @G1FN@<double, double, NT>(c, o, sm); } static constexpr int SLOTS = @G1SLOTS@; };
+
+template <class F>
+__global__ void __launch_bounds__(128, 1) kern_global(RfmArrays rfm, const double *in, double *out) {
+  const int i0 = NG + blockIdx.x * 32 + threadIdx.x, i1 = NG + blockIdx.y * 4 + threadIdx.y, i2 = NG + blockIdx.z;
+  extern __shared__ double smem[];
+  volatile double *sm = smem + threadIdx.x + 32 * threadIdx.y;
+  const int idx = i0 + N0 * i1 + N0 * N1 * i2;
+  PointCtx ctx;
+  ctx.in = in + idx; ctx.aux = nullptr; ctx.s1 = N0; ctx.s2 = N0 * N1; ctx.ntot = NTOT; ctx.i0 = i0; ctx.i1 = i1;
+  ctx.invdxx0 = 10.0; ctx.invdxx1 = 20.0; ctx.invdxx2 = 5.0; ctx.rfm = rfm;
+  double o[3];
+  F::template eval<128>(ctx, o, sm);
+  for (int k = 0; k < 3; k++) out[idx + k * NTOT] = o[k];
+}
+
+template <int TX, int TY, int TZ, class F>
+__global__ void __launch_bounds__(TX * TY * TZ, 1) kern_staged(RfmArrays rfm, const double *in, double *out) {
+  constexpr int NT = TX * TY * TZ, SX = TX + 4, SY = TY + 4, SZ = TZ + 4, BOX = SX * SY * SZ;
+  extern __shared__ double smem[];
+  const int tid = threadIdx.x + TX * (threadIdx.y + TY * threadIdx.z);
+  const int o0 = NG + blockIdx.x * TX - 2, o1 = NG + blockIdx.y * TY - 2, o2 = NG + blockIdx.z * TZ - 2;
+  for (int e = tid; e < 9 * BOX; e += NT) {
+    const int g = e / BOX, r = e - g * BOX;
+    const int z = r / (SX * SY), r2 = r - z * (SX * SY);
+    const int y = r2 / SX, x = r2 - y * SX;
+    const int j0 = o0 + x, j1 = o1 + y, j2 = o2 + z;
+    smem[e] = (j0 < N0 && j1 < N1 && j2 < N2) ? __ldg(in + (size_t)(11 + g) * NTOT + j0 + N0 * (j1 + N1 * j2)) : 0.0;
+  }
+  __syncthreads();
+  const int i0 = NG + blockIdx.x * TX + threadIdx.x, i1 = NG + blockIdx.y * TY + threadIdx.y, i2 = NG + blockIdx.z * TZ + threadIdx.z;
+  volatile double *sm = smem + 9 * BOX + tid;
+  SmemCtx<SX, SY, SZ> ctx;
+  ctx.s = smem + ((threadIdx.z + 2) * SY + (threadIdx.y + 2)) * SX + (threadIdx.x + 2);
+  ctx.i0 = i0; ctx.i1 = i1;
+  ctx.invdxx0 = 10.0; ctx.invdxx1 = 20.0; ctx.invdxx2 = 5.0; ctx.rfm = rfm;
+  double o[3];
+  F::template eval<NT>(ctx, o, sm);
+  const int idx = i0 + N0 * i1 + N0 * N1 * i2;
+  for (int k = 0; k < 3; k++) out[idx + k * NTOT] = o[k];
+}
+
+template <class K>
+float time_kernel(K k, dim3 grid, dim3 block, size_t sb, RfmArrays rfm, const double *in, double *out, const char *name) {
+  if (sb > 227 * 1024) { printf("{\"kernel\": \"%s\", \"skip\": \"smem %zu\"}\n", name, sb); return -1; }
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sb);
+  cudaFuncAttributes at; cudaFuncGetAttributes(&at, k);
+  int nb = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, block.x * block.y * block.z, sb);
+  cudaEvent_t a, b; cudaEventCreate(&a); cudaEventCreate(&b);
+  for (int w = 0; w < 2; w++) k<<<grid, block, sb>>>(rfm, in, out);
+  std::vector<float> ts;
+  for (int r = 0; r < 7; r++) {
+    cudaEventRecord(a); k<<<grid, block, sb>>>(rfm, in, out); cudaEventRecord(b); cudaEventSynchronize(b);
+    float ms; cudaEventElapsedTime(&ms, a, b); ts.push_back(ms);
+  }
+  std::sort(ts.begin(), ts.end());
+  const cudaError_t e = cudaGetLastError();
+  printf("{\"kernel\": \"%s\", \"regs\": %d, \"local\": %zu, \"smem\": %zu, \"warps_per_sm\": %d, \"us\": %.1f, \"error\": \"%s\"}\n",
+         name, at.numRegs, at.localSizeBytes, sb, nb * (int)(block.x * block.y * block.z) / 32, ts[3] * 1e3,
+         e == cudaSuccess ? "" : cudaGetErrorString(e));
+  return ts[3];
+}
+
+template <int TX, int TY, int TZ, class F>
+void staged(const char *name, RfmArrays rfm, const double *in, double *out, const std::vector<double> &ref) {
+  constexpr int BOX = (TX + 4) * (TY + 4) * (TZ + 4);
+  const size_t sb = (size_t)(9 * BOX + F::SLOTS * TX * TY * TZ) * 8;
+  cudaMemset(out, 0, (size_t)NTOT * 3 * 8);
+  time_kernel(kern_staged<TX, TY, TZ, F>, dim3(256 / TX, 64 / TY, 32 / TZ), dim3(TX, TY, TZ), sb, rfm, in, out, name);
+  std::vector<double> h((size_t)NTOT * 3);
+  cudaMemcpy(h.data(), out, h.size() * 8, cudaMemcpyDeviceToHost);
+  double md = 0, mr = 0;
+  for (int i2 = NG; i2 < N2 - NG; i2++) for (int i1 = NG; i1 < N1 - NG; i1++) for (int i0 = NG; i0 < N0 - NG; i0++)
+    for (int k = 0; k < 3; k++) { const size_t q = i0 + N0 * (i1 + (size_t)N1 * i2) + (size_t)k * NTOT;
+      md = std::max(md, std::abs(h[q] - ref[q])); mr = std::max(mr, std::abs(ref[q])); }
+  printf("{\"kernel\": \"%s\", \"max_abs_diff_vs_global\": %.3e, \"max_abs\": %.3e}\n", name, md, mr);
+}
+
+template <class F>
+void both(const char *gname, RfmArrays rfm, const double *in, double *out) {
+  char nm[64];
+  snprintf(nm, sizeof nm, "%s_global", gname);
+  time_kernel(kern_global<F>, dim3(8, 16, 32), dim3(32, 4, 1), (size_t)F::SLOTS * 128 * 8, rfm, in, out, nm);
+  std::vector<double> ref((size_t)NTOT * 3);
+  cudaMemcpy(ref.data(), out, ref.size() * 8, cudaMemcpyDeviceToHost);
+  snprintf(nm, sizeof nm, "%s_staged_32x4x1", gname); staged<32, 4, 1, F>(nm, rfm, in, out, ref);
+  snprintf(nm, sizeof nm, "%s_staged_32x4x2", gname); staged<32, 4, 2, F>(nm, rfm, in, out, ref);
+  snprintf(nm, sizeof nm, "%s_staged_16x8x2", gname); staged<16, 8, 2, F>(nm, rfm, in, out, ref);
+  snprintf(nm, sizeof nm, "%s_staged_16x4x2", gname); staged<16, 4, 2, F>(nm, rfm, in, out, ref);
+  snprintf(nm, sizeof nm, "%s_staged_32x2x2", gname); staged<32, 2, 2, F>(nm, rfm, in, out, ref);
+  snprintf(nm, sizeof nm, "%s_staged_16x4x4", gname); staged<16, 4, 4, F>(nm, rfm, in, out, ref);
+}
+
+int main() {
+  std::vector<double> h((size_t)NTOT * 24);
+  srand(7);
+  for (auto &x : h) x = 0.5 + (double)rand() / RAND_MAX;
+  double *in, *out, *r[7];
+  cudaMalloc(&in, h.size() * 8);
+  cudaMemcpy(in, h.data(), h.size() * 8, cudaMemcpyHostToDevice);
+  cudaMalloc(&out, (size_t)NTOT * 3 * 8);
+  for (int k = 0; k < 7; k++) {
+    cudaMalloc(&r[k], 300 * 8);
+    cudaMemcpy(r[k], h.data() + 1000 * k, 300 * 8, cudaMemcpyHostToDevice);
+  }
+  RfmArrays rfm{r[0], r[1], r[2], r[3], r[4], r[5], r[6]};
+  both<G0>("ricci_g0", rfm, in, out);
+  both<G1>("ricci_g1", rfm, in, out);
+  return 0;
+}
+'''
+
+
+def generate_staged() -> None:
+    """The present Ricci groups (allocation and budget of generate.py) reading their nine
+    stencil gridfunctions (hDD, lambdaU; radius 2) from a shared-memory copy of the block's
+    tile plus a 2-point halo, filled by the block before it evaluates, against the same
+    groups reading global memory. Tiles 32x4x1 to 16x4x4 points; the harness checks that
+    both forms give the same values."""
+    from nrpy_b200.codegen import bssn_exprs as be
+    from nrpy_b200.codegen.emit_cuda import emit_point_function
+    from nrpy_b200.codegen.generate import RICCI_ALLOC, RICCI_CAPS
+
+    be.setup_nrpy("")
+    ricci = be.ricci_exprs("SinhSpherical")
+    OUT.mkdir(parents=True, exist_ok=True)
+    parts, sub = ["#pragma once\n"], {}
+    for g, gname in enumerate(("ricci_012", "ricci_345")):
+        names = CANDIDATES[gname][1]
+        rf, dr, order = RICCI_ALLOC[g]
+        fname = f"{gname}_c{RICCI_CAPS[g]}"
+        code, st = emit_point_function(fname, [(f"out[{i}]", ricci[n]) for i, n in enumerate(names)],
+                                       reg_capacity=RICCI_CAPS[g], remat_first=rf, deriv_remat=dr, order=order)
+        parts.append(code)
+        sub[f"@G{g}FN@"] = fname
+        sub[f"@G{g}SLOTS@"] = str(max(st["smem_slots"], 1))
+    (OUT / "staged_ricci.cuh").write_text("\n".join(parts))
+    src = STAGED_HARNESS
+    for k, v in sub.items():
+        src = src.replace(k, v)
+    (OUT / "staged_ricci.cu").write_text(src)
+    print("staged_ricci", sub, flush=True)
+
+
 def compile_all(jobs: int) -> None:
     from nrpy_b200.build import nvcc
 
@@ -380,8 +569,8 @@ def summarize(path: str) -> None:
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("step", choices=["generate", "generate-orders", "generate-caps", "generate-leaf", "compile", "run",
-                                     "summarize"])
+    ap.add_argument("step", choices=["generate", "generate-orders", "generate-caps", "generate-leaf",
+                                     "generate-staged", "compile", "run", "summarize"])
     ap.add_argument("--caps", default="72,80,90,100")
     ap.add_argument("--fd-order", type=int, default=4)
     ap.add_argument("--dtype", default="double", choices=["double", "float"], help="value type of generate-caps")
@@ -397,6 +586,8 @@ if __name__ == "__main__":
         generate_caps([int(c) for c in a.caps.split(",")], a.fd_order, a.dtype, [g for g in a.groups.split(",") if g])
     elif a.step == "generate-leaf":
         generate_leaf()
+    elif a.step == "generate-staged":
+        generate_staged()
     elif a.step == "compile":
         compile_all(a.jobs)
     elif a.step == "run":
