@@ -35,6 +35,9 @@ def grid_params(coord: str, Nxx, grid_physical_size: float, sinhw: float = 0.2) 
     elif coord == "Spherical":
         p["RMAX"] = grid_physical_size
         xmin, xmax = [0.0, 0.0, -PI], [grid_physical_size, PI, PI]
+    elif coord == "SinhCylindrical":
+        p["AMPLRHO"] = p["AMPLZ"] = grid_physical_size
+        xmin, xmax = [0.0, -PI, -1.0], [1.0, PI, 1.0]
     else:
         raise ValueError(coord)
     p["N"] = tuple(n + 2 * NGHOSTS for n in Nxx)
@@ -73,13 +76,19 @@ def cfl_dt(p: Dict, cfl: float = 0.5) -> float:
 # ------------------------------------------------------------------------ bcstruct
 def _eigen_map(p: Dict, i0: int, i1: int, i2: int) -> Tuple[Tuple[int, int, int], Tuple[float, float, float]]:
     """EigenCoord_set_x0x1x2_inbounds__i0i1i2_inbounds_single_pt (bcstruct_set_up.py:195-440):
-    (x0,x1,x2) -> Cartesian in the eigen-coordinate (Spherical) -> (x0,x1,x2)' -> nearest index."""
+    (x0,x1,x2) -> Cartesian in the eigen-coordinate (Spherical, or Cylindrical for the
+    cylindrical family: the xx values are taken as the eigen coordinates themselves) ->
+    (x0,x1,x2)' -> nearest index."""
     xx = p["xx"]
     x0, x1, x2 = xx[0][i0], xx[1][i1], xx[2][i2]
-    t = x0 * math.sin(x1)
-    X, Y, Z = t * math.cos(x2), t * math.sin(x2), x0 * math.cos(x1)
-    r = math.sqrt(X * X + Y * Y + Z * Z)
-    xin = (r, math.acos(Z / r), math.atan2(Y, X))
+    if p["coord"] == "SinhCylindrical":
+        X, Y, Z = x0 * math.cos(x1), x0 * math.sin(x1), x2
+        xin = (math.sqrt(X * X + Y * Y), math.atan2(Y, X), Z)
+    else:
+        t = x0 * math.sin(x1)
+        X, Y, Z = t * math.cos(x2), t * math.sin(x2), x0 * math.cos(x1)
+        r = math.sqrt(X * X + Y * Y + Z * Z)
+        xin = (r, math.acos(Z / r), math.atan2(Y, X))
     idx = []
     for d in range(3):
         dx = p["dxx"][d]
@@ -88,8 +97,17 @@ def _eigen_map(p: Dict, i0: int, i1: int, i2: int) -> Tuple[Tuple[int, int, int]
     return tuple(idx), tuple(xx[d][idx[d]] for d in range(3))
 
 
-def _parity(x1: float, x2: float, xin) -> List[int]:
-    """set_parity_for_inner_boundary_single_pt (bcstruct_set_up.py:38-190): unit-vector dot products."""
+def _parity(x1: float, x2: float, xin, coord: str = "Spherical") -> List[int]:
+    """set_parity_for_inner_boundary_single_pt (bcstruct_set_up.py:38-190): unit-vector dot products
+    of the point and its source, in the eigen basis (Spherical; Cylindrical: rho-hat and phi-hat
+    turn with the phi difference, z-hat does not)."""
+    if coord == "SinhCylindrical":
+        t = math.sin(x1) * math.sin(xin[1]) + math.cos(x1) * math.cos(xin[1])
+        vals = [1.0, t, t, 1.0, t * t, t * t, t, t * t, t, 1.0]
+        for v in vals:
+            if abs(v) < 1 - 1e-8 or abs(v) > 1 + 1e-8:
+                raise ValueError(f"parity {v} not +/-1")
+        return [-1 if v < 0 else 1 for v in vals]
     y1, y2 = xin[1], xin[2]
     a = math.cos(x1) * math.cos(y1)
     b = math.sin(x1) * math.sin(y1)
@@ -119,7 +137,7 @@ def bcstruct(p: Dict):
                 if (j0, j1, j2) == (i0, i1, i2):
                     continue
                 inner.append((i0 + N0 * (i1 + N1 * i2), j0 + N0 * (j1 + N1 * j2),
-                              _parity(p["xx"][1][i1], p["xx"][2][i2], xin)))
+                              _parity(p["xx"][1][i1], p["xx"][2][i2], xin, p["coord"])))
     imin = [NGHOSTS] * 3
     imax = [N0 - NGHOSTS, N1 - NGHOSTS, N2 - NGHOSTS]
     bounds = []

@@ -74,3 +74,24 @@ def compare_diagnostics_dirs(ref_dir: pathlib.Path, ours_dir: pathlib.Path) -> l
         scale = np.abs(d_ref[:, nc:]).max(axis=0)
         assert np.all(np.abs(d_ours[:, nc:] - d_ref[:, nc:]) <= 1e-9 * scale + 1e-300), name
     return names
+
+
+# The SENR inner-boundary known-answer files (tests/golden/senr_kat.npz, made by
+# tests/golden/make_senr_kat.py) list ten gridfunctions in SENR's order: vet^1..3, a_11, a_12,
+# a_13, a_22, a_23, a_33, cf. Their parity types in the reference's numbering (0 scalar, 1-3
+# vector components, 4-9 the symmetric rank-2 components 00, 01, 02, 11, 12, 22):
+SENR_PARITY_TYPE = [1, 2, 3, 4, 5, 6, 7, 8, 9, 0]
+
+
+def senr_kat_values(inner, ijk: np.ndarray, n: int = 10) -> np.ndarray:
+    """The KAT's printed values predicted from an inner-boundary list of (dstpt, srcpt, parity[10])
+    on an n^3 grid: gridfunction g at point p holds 1000 g + index(p), and after the inner BCs a
+    ghost point holds parity[type(g)] * (1000 g + index(source))."""
+    src = {int(d): (int(s), [int(x) for x in par]) for d, s, par in inner}
+    out = np.empty((len(ijk), 10), dtype=np.int64)
+    for row, (i, j, k) in enumerate(ijk):
+        p = int(i) + n * (int(j) + n * int(k))
+        s, par = src.get(p, (p, [1] * 10))
+        for g in range(10):
+            out[row, g] = par[SENR_PARITY_TYPE[g]] * (1000 * g + s)
+    return out
