@@ -192,7 +192,11 @@ static int batch_build(bssn_b200_batch *b) {
       for (const auto &q : h) inner.push_back(BatchInnerPt{e, q});
     }
   }
-  b->ntiles = (int)std::min<long long>(ntiles, 1LL << 30);
+  if (ntiles > (1LL << 30)) {
+    set_error("batch: %lld tiles in all, more than 2^30", ntiles);
+    return BSSN_B200_EINVAL;
+  }
+  b->ntiles = (int)ntiles;
   BSSN_TRY(upload(&b->d_descs, descs));
   for (int gz = 0; gz < NGHOSTS; gz++) {
     b->nouter_layer[gz] = (int)layer[gz].size();

@@ -30,8 +30,8 @@ Variants
            for sm_100a (relocatable device code, the generated Makefile's flags with
            ``-arch=sm_100a``) together with ``oracle/ref_harness_cuda.cu`` into
            ``oracle/_ref/sinh3d_cuda/libref_cuda.so``: the reference's own GPU step, timed
-           beside this library's on the B200 (not part of the default variant list; it needs
-           nvcc, not a GPU, to build)
+           beside this library's on the B200 (built by default after the C variants; it
+           needs nvcc, not a GPU, to build)
 
 Usage: python oracle/gen_ref.py [--variants sphaxi,sph3d,sinh3d,sinh3d_cuda] [--reference DIR]
 """
@@ -156,7 +156,7 @@ def compile_cuda_variant(variant: str, proj: pathlib.Path, jobs: int) -> None:
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--variants", default=",".join(VARIANTS))
+    ap.add_argument("--variants", default=",".join(list(VARIANTS) + list(CUDA_VARIANTS)))
     ap.add_argument("--reference", default=os.environ.get("NRPY_REFERENCE", str(HERE.parent.parent / "reference")),
                     help="the nrpy checkout (default: $NRPY_REFERENCE, else ../reference beside this repository)")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)

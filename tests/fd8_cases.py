@@ -23,6 +23,7 @@ from tests.sinhcyl_cases import (  # noqa: F401  (SinhCylindrical at 8th order: 
     test_sinhcyl_20_steps,
     test_sinhcyl_brill_lindquist_50_steps,
     test_sinhcyl_diagnostics_files,
+    test_sinhcyl_dt_matches_reference,
     test_sinhcyl_grid_bcstruct_and_initial_data,
     test_sinhcyl_ricci_rhs_constraints,
 )

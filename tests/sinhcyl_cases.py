@@ -94,6 +94,22 @@ def test_sinhcyl_grid_bcstruct_and_initial_data(cuda):
     g.close()
 
 
+def test_sinhcyl_dt_matches_reference(cuda):
+    """The CFL timestep equals the reference's bit for bit on grids whose smallest spacing lies
+    along z (where the reference's compiled z' sum is a fused multiply-add) and along rho."""
+    from nrpy_b200.grid import BSSNGrid
+
+    _, variant = _ng()
+    if not oref.available(variant):
+        pytest.skip(f"oracle/_ref/{variant} not built")
+    for nxx, L in [((40, 2, 120), 10.0), ((40, 2, 64), 30.0), ((40, 2, 120), 30.0), ((64, 2, 40), 10.0)]:
+        rg = oref.RefGrid(variant, nxx, L, SINHW=0.2)
+        g = BSSNGrid(coord="SinhCylindrical", Nxx=nxx, grid_physical_size=L, SINHW=0.2, symmetry_axes="1")
+        assert g.dt == rg.dt, (nxx, L, g.dt, rg.dt)
+        rg.close()
+        g.close()
+
+
 def test_sinhcyl_ricci_rhs_constraints(cuda):
     rg, g, ng = _pair()
     inp = oref.perturbed_state(rg, seed=5, amp=0.03)
