@@ -556,8 +556,12 @@ def emit_point_function(
     deriv_remat: bool = False,
     order: str = "dfs",
     leaf_index: Optional[Dict[str, int]] = None,
+    prefetch_rows: int = 0,
 ) -> Tuple[str, Dict[str, int]]:
-    """Emit `fname` and the constant `fname_SMEM_SLOTS`. With reg_capacity > 0 the values
+    """Emit `fname` and the constant `fname_SMEM_SLOTS`. With prefetch_rows = D > 0, each
+    stencil row (gridfunction, i1 offset, i2 offset) is prefetched into L1
+    (PREFETCH_ROW(gf, b, c), provided by the caller's context) D statements before the
+    statement that first loads from it. With reg_capacity > 0 the values
     beyond that many live doubles go to shared-memory slots (SMEM(k), provided by the
     caller through the `sm` argument: slot k of this thread; the template parameter NT is
     the slot stride, i.e. the threads of a block). The slot pointer type S is the caller's:
@@ -573,6 +577,8 @@ def emit_point_function(
         lines, nslots = allocate_values(ordered, reg_capacity, remat_first, deriv_remat)
     else:
         lines, nslots = pk.lines, 0
+    if prefetch_rows > 0:
+        lines = insert_row_prefetches(lines, prefetch_rows)
     body = "\n".join("  " + ln for ln in lines)
     head = f"// {comment}\n" if comment else ""
     code = (
@@ -584,6 +590,29 @@ def emit_point_function(
     stats = dict(pk.stats)
     stats["smem_slots"] = nslots
     return code, stats
+
+
+_LD_RE = re.compile(r"LD\((\d+), *(-?\d+), *(-?\d+), *(-?\d+)\)")
+
+
+def insert_row_prefetches(lines: Sequence[str], distance: int) -> List[str]:
+    """Insert PREFETCH_ROW(gf, b, c) `distance` statements before the first statement that
+    loads from stencil row (gf, b, c); rows first loaded within the first `distance`
+    statements are prefetched at the top, in the order of their first loads."""
+    first = {}
+    for k, ln in enumerate(lines):
+        for m in _LD_RE.finditer(ln):
+            key = (int(m.group(1)), int(m.group(3)), int(m.group(4)))
+            first.setdefault(key, k)
+    at = {}
+    for key, k in first.items():
+        at.setdefault(max(0, k - distance), []).append(key)
+    out = []
+    for k, ln in enumerate(lines):
+        for gf, b, c in at.get(k, []):
+            out.append(f"PREFETCH_ROW({gf}, {b}, {c});")
+        out.append(ln)
+    return out
 
 
 def leaf_names(exprs: Sequence[sp.Expr]) -> List[str]:

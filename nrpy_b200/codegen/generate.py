@@ -68,6 +68,15 @@ RHS_CAPS = [72, 80]
 # (budget 250); RHS group 1 171 -> 160 us at budget 200; RHS group 0 was fastest at 72.
 RICCI_CAPS_F32 = [250, 250]
 RHS_CAPS_F32 = [72, 200]
+# Statements between an L1 prefetch of a stencil row and its first load, per group (0: no
+# prefetch), in the FP64 and the FP32 evaluation. Timed on the bench workload (SinhSpherical
+# 256x64x64, mixed precision): RHS group 0 in FP32 at distances 25-100 gave 154.9-175.0 M
+# pt-updates/s against 156.7 M without, best at 52-55 (174.3-175.0 M); a prefetch in RHS
+# group 1 or in the Ricci groups gave nothing or lost.
+RICCI_PREFETCH = [0, 0]
+RHS_PREFETCH = [0, 0]
+RICCI_PREFETCH_F32 = [0, 0]
+RHS_PREFETCH_F32 = [55, 0]
 # Value types for which a group's slot array is plain instead of volatile (volatile: every slot
 # access stays where the allocator put it; plain: the compiler may schedule the accesses), per
 # group, from a timing sweep: plain slots help the RHS groups in FP32 and cost in FP64.
@@ -159,15 +168,17 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
             fname, [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
             comment=f"Rbar_ij {names}, {coord} (symmetry_axes='{sym}'): Ricci_eval.py:27-167",
             reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+            prefetch_rows=RICCI_PREFETCH[g],
         )
         parts.append(code)
         stats[f"ricci_g{g}"] = st
         f32 = {}
-        if RICCI_CAPS_F32[g] != cap:
+        if RICCI_CAPS_F32[g] != cap or RICCI_PREFETCH_F32[g] != RICCI_PREFETCH[g]:
             code, st32 = emit_point_function(
                 fname + "_f32", [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
                 comment=f"Rbar_ij {names}, {coord}: the FP32 evaluation's allocation",
                 reg_capacity=RICCI_CAPS_F32[g], remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+                prefetch_rows=RICCI_PREFETCH_F32[g],
             )
             parts.append(code)
             stats[f"ricci_g{g}_f32"] = st32
@@ -182,15 +193,17 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
             fname, [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU, symmetry_axes=sym,
             comment=f"BSSN RHS + KO (CAKO) of {names}, {coord} (symmetry_axes='{sym}'): rhs_eval.py:122-220",
             reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+            prefetch_rows=RHS_PREFETCH[g],
         )
         parts.append(code)
         stats[f"rhs_g{g}"] = st
         f32 = {}
-        if RHS_CAPS_F32[g] != cap:
+        if RHS_CAPS_F32[g] != cap or RHS_PREFETCH_F32[g] != RHS_PREFETCH[g]:
             code, st32 = emit_point_function(
                 fname + "_f32", [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU,
                 symmetry_axes=sym, comment=f"BSSN RHS + KO (CAKO) of {names}, {coord}: the FP32 evaluation's allocation",
                 reg_capacity=RHS_CAPS_F32[g], remat_first=remat_first, deriv_remat=deriv_remat, order=order,
+                prefetch_rows=RHS_PREFETCH_F32[g],
             )
             parts.append(code)
             stats[f"rhs_g{g}_f32"] = st32
@@ -230,7 +243,9 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
         "// Generated by nrpy_b200/codegen/generate.py from NRPy's BSSN equation modules.\n"
         f"// Variant {tag}: CoordSystem={coord}, symmetry_axes='{sym}', {fd_order}th-order FD, KO (CAKO).\n"
         f"// Register budgets Ricci {RICCI_CAPS}, RHS {RHS_CAPS} values (FP32 evaluation: Ricci {RICCI_CAPS_F32}, "
-        f"RHS {RHS_CAPS_F32}); allocation (remat_first, deriv_remat, "
+        f"RHS {RHS_CAPS_F32}); L1 row prefetch distance Ricci {RICCI_PREFETCH}, RHS {RHS_PREFETCH} (FP32: "
+        f"Ricci {RICCI_PREFETCH_F32}, RHS {RHS_PREFETCH_F32}); "
+        f"allocation (remat_first, deriv_remat, "
         f"order): Ricci {RICCI_ALLOC}, RHS {RHS_ALLOC}; plain slots Ricci {RICCI_PLAIN_SLOTS}, RHS {RHS_PLAIN_SLOTS}.\n"
         f"// Per point: {stats}\n"
         "#pragma once\n\n"
@@ -372,9 +387,20 @@ def main() -> None:
     ap.add_argument("--adjoint", default=",".join(ADJOINT_VARIANTS))
     ap.add_argument("--fd-order", type=int, default=4,
                     help="interior FD order of the forward variants (the adjoint is 4th order only)")
+    ap.add_argument("--prefetch-f32", default=None,
+                    help="tuning: L1 row-prefetch distances of the FP32 groups, 'ricci0,ricci1,rhs0,rhs1'")
+    ap.add_argument("--prefetch-f64", default=None, help="tuning: the same for the FP64 groups")
     ap.add_argument("--one", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--one-adjoint", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.prefetch_f32:
+        d = [int(x) for x in args.prefetch_f32.split(",")]
+        RICCI_PREFETCH_F32[:] = d[:2]
+        RHS_PREFETCH_F32[:] = d[2:4]
+    if args.prefetch_f64:
+        d = [int(x) for x in args.prefetch_f64.split(",")]
+        RICCI_PREFETCH[:] = d[:2]
+        RHS_PREFETCH[:] = d[2:4]
     if args.one:
         generate_variant(args.one, args.fd_order)
         return
@@ -386,7 +412,9 @@ def main() -> None:
     env["PYTHONPATH"] = f"{ROOT}:{shim}:{args.reference}"
     procs = [
         subprocess.Popen([sys.executable, "-m", "nrpy_b200.codegen.generate", "--one", tag, "--fd-order",
-                          str(args.fd_order)], env=env, cwd=ROOT)
+                          str(args.fd_order)] + (["--prefetch-f32", args.prefetch_f32] if args.prefetch_f32 else [])
+                         + (["--prefetch-f64", args.prefetch_f64] if args.prefetch_f64 else []),
+                         env=env, cwd=ROOT)
         for tag in args.variants.split(",") if tag
     ]
     if args.fd_order != 4 and args.adjoint:

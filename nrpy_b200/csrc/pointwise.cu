@@ -35,6 +35,10 @@ struct PointCtx {
     return __ldg(in + (gf * ntot + (a + b * s1 + c * s2)));
   }
   __device__ __forceinline__ double ldaux(int k) const { return __ldg(aux + k * ntot); }
+  // L1 prefetch of the line holding stencil point (0, b, c) of gridfunction gf.
+  __device__ __forceinline__ void prefetch_row(int gf, int b, int c) const {
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(in + (gf * ntot + (b * s1 + c * s2))));
+  }
 };
 
 // Point values held in registers (pointwise operators without stencils).
@@ -47,6 +51,7 @@ struct RegCtx {
 
 #define LD(gf, a, b, c) ctx.ld(gf, a, b, c)
 #define LDAUX(k) ctx.ldaux(k)
+#define PREFETCH_ROW(gf, b, c) ctx.prefetch_row(gf, b, c)
 #define RFM(arr, d) __ldg(ctx.rfm.arr + ctx.i##d)
 #define rfm_f0 f0
 #define rfm_f0_D0 f0_D0
