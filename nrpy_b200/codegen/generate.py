@@ -73,10 +73,13 @@ RHS_CAPS_F32 = [72, 200]
 # 256x64x64, mixed precision): RHS group 0 in FP32 at distances 25-100 gave 154.9-175.0 M
 # pt-updates/s against 156.7 M without, best at 52-55 (174.3-175.0 M); a prefetch in RHS
 # group 1 or in the Ricci groups gave nothing or lost.
+# At 8th order the same FP32 prefetch lost (mixed 67.5 -> 65.6 M at 256x64x64), so the
+# distances apply to 4th order; other orders get none unless --prefetch-f32/-f64 says so.
 RICCI_PREFETCH = [0, 0]
 RHS_PREFETCH = [0, 0]
 RICCI_PREFETCH_F32 = [0, 0]
 RHS_PREFETCH_F32 = [55, 0]
+PREFETCH_FD_ORDER = 4
 # Value types for which a group's slot array is plain instead of volatile (volatile: every slot
 # access stays where the allocator put it; plain: the compiler may schedule the accesses), per
 # group, from a timing sweep: plain slots help the RHS groups in FP32 and cost in FP64.
@@ -150,6 +153,9 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
     from nrpy_b200.codegen.emit_cuda import emit_point_function
 
     coord, sym = VARIANTS[tag]
+    if fd_order != PREFETCH_FD_ORDER:
+        for lst in (RICCI_PREFETCH, RHS_PREFETCH, RICCI_PREFETCH_F32, RHS_PREFETCH_F32):
+            lst[:] = [0] * len(lst)
     fdc.set_fd_order(fd_order)
     be.setup_nrpy(sym, fd_order)
     t0 = time.time()
@@ -393,6 +399,11 @@ def main() -> None:
     ap.add_argument("--one", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--one-adjoint", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    global PREFETCH_FD_ORDER
+    if args.prefetch_f32 or args.prefetch_f64:
+        PREFETCH_FD_ORDER = args.fd_order  # explicit distances hold for the order being generated
+        for lst in (RICCI_PREFETCH, RHS_PREFETCH, RICCI_PREFETCH_F32, RHS_PREFETCH_F32):
+            lst[:] = [0] * len(lst)
     if args.prefetch_f32:
         d = [int(x) for x in args.prefetch_f32.split(",")]
         RICCI_PREFETCH_F32[:] = d[:2]
