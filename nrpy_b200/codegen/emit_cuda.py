@@ -557,6 +557,7 @@ def emit_point_function(
     order: str = "dfs",
     leaf_index: Optional[Dict[str, int]] = None,
     prefetch_rows: int = 0,
+    prefetch_macro: str = "PREFETCH_ROW",
 ) -> Tuple[str, Dict[str, int]]:
     """Emit `fname` and the constant `fname_SMEM_SLOTS`. With prefetch_rows = D > 0, each
     stencil row (gridfunction, i1 offset, i2 offset) is prefetched into L1
@@ -578,7 +579,7 @@ def emit_point_function(
     else:
         lines, nslots = pk.lines, 0
     if prefetch_rows > 0:
-        lines = insert_row_prefetches(lines, prefetch_rows)
+        lines = insert_row_prefetches(lines, prefetch_rows, prefetch_macro)
     body = "\n".join("  " + ln for ln in lines)
     head = f"// {comment}\n" if comment else ""
     code = (
@@ -595,7 +596,7 @@ def emit_point_function(
 _LD_RE = re.compile(r"LD\((\d+), *(-?\d+), *(-?\d+), *(-?\d+)\)")
 
 
-def insert_row_prefetches(lines: Sequence[str], distance: int) -> List[str]:
+def insert_row_prefetches(lines: Sequence[str], distance: int, macro: str = "PREFETCH_ROW") -> List[str]:
     """Insert PREFETCH_ROW(gf, b, c) `distance` statements before the first statement that
     loads from stencil row (gf, b, c); rows first loaded within the first `distance`
     statements are prefetched at the top, in the order of their first loads."""
@@ -610,7 +611,7 @@ def insert_row_prefetches(lines: Sequence[str], distance: int) -> List[str]:
     out = []
     for k, ln in enumerate(lines):
         for gf, b, c in at.get(k, []):
-            out.append(f"PREFETCH_ROW({gf}, {b}, {c});")
+            out.append(f"{macro}({gf}, {b}, {c});")
         out.append(ln)
     return out
 

@@ -80,6 +80,8 @@ RHS_PREFETCH = [0, 0]
 RICCI_PREFETCH_F32 = [0, 0]
 RHS_PREFETCH_F32 = [55, 0]
 PREFETCH_FD_ORDER = 4
+# Prefetch statement of the FP64 groups: PREFETCH_ROW (L1) or PREFETCH_ROW_L2.
+PREFETCH_MACRO = "PREFETCH_ROW"
 # Value types for which a group's slot array is plain instead of volatile (volatile: every slot
 # access stays where the allocator put it; plain: the compiler may schedule the accesses), per
 # group, from a timing sweep: plain slots help the RHS groups in FP32 and cost in FP64.
@@ -174,7 +176,7 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
             fname, [(f"out[{i}]", ricci[k]) for i, k in enumerate(names)], symmetry_axes=sym,
             comment=f"Rbar_ij {names}, {coord} (symmetry_axes='{sym}'): Ricci_eval.py:27-167",
             reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
-            prefetch_rows=RICCI_PREFETCH[g],
+            prefetch_rows=RICCI_PREFETCH[g], prefetch_macro=PREFETCH_MACRO,
         )
         parts.append(code)
         stats[f"ricci_g{g}"] = st
@@ -199,7 +201,7 @@ def generate_variant(tag: str, fd_order: int = 4) -> None:
             fname, [(f"out[{i}]", rhs[k]) for i, k in enumerate(names)], upwind_vec=betaU, symmetry_axes=sym,
             comment=f"BSSN RHS + KO (CAKO) of {names}, {coord} (symmetry_axes='{sym}'): rhs_eval.py:122-220",
             reg_capacity=cap, remat_first=remat_first, deriv_remat=deriv_remat, order=order,
-            prefetch_rows=RHS_PREFETCH[g],
+            prefetch_rows=RHS_PREFETCH[g], prefetch_macro=PREFETCH_MACRO,
         )
         parts.append(code)
         stats[f"rhs_g{g}"] = st
@@ -396,6 +398,7 @@ def main() -> None:
     ap.add_argument("--prefetch-f32", default=None,
                     help="tuning: L1 row-prefetch distances of the FP32 groups, 'ricci0,ricci1,rhs0,rhs1'")
     ap.add_argument("--prefetch-f64", default=None, help="tuning: the same for the FP64 groups")
+    ap.add_argument("--prefetch-f64-l2", action="store_true", help="tuning: FP64 row prefetches into L2")
     ap.add_argument("--one", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--one-adjoint", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -408,6 +411,9 @@ def main() -> None:
         d = [int(x) for x in args.prefetch_f32.split(",")]
         RICCI_PREFETCH_F32[:] = d[:2]
         RHS_PREFETCH_F32[:] = d[2:4]
+    global PREFETCH_MACRO
+    if args.prefetch_f64_l2:
+        PREFETCH_MACRO = "PREFETCH_ROW_L2"
     if args.prefetch_f64:
         d = [int(x) for x in args.prefetch_f64.split(",")]
         RICCI_PREFETCH[:] = d[:2]
@@ -424,7 +430,8 @@ def main() -> None:
     procs = [
         subprocess.Popen([sys.executable, "-m", "nrpy_b200.codegen.generate", "--one", tag, "--fd-order",
                           str(args.fd_order)] + (["--prefetch-f32", args.prefetch_f32] if args.prefetch_f32 else [])
-                         + (["--prefetch-f64", args.prefetch_f64] if args.prefetch_f64 else []),
+                         + (["--prefetch-f64", args.prefetch_f64] if args.prefetch_f64 else [])
+                         + (["--prefetch-f64-l2"] if args.prefetch_f64_l2 else []),
                          env=env, cwd=ROOT)
         for tag in args.variants.split(",") if tag
     ]

@@ -39,6 +39,9 @@ struct PointCtx {
   __device__ __forceinline__ void prefetch_row(int gf, int b, int c) const {
     asm volatile("prefetch.global.L1 [%0];" ::"l"(in + (gf * ntot + (b * s1 + c * s2))));
   }
+  __device__ __forceinline__ void prefetch_row_l2(int gf, int b, int c) const {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(in + (gf * ntot + (b * s1 + c * s2))));
+  }
 };
 
 // Point values held in registers (pointwise operators without stencils).
@@ -52,6 +55,7 @@ struct RegCtx {
 #define LD(gf, a, b, c) ctx.ld(gf, a, b, c)
 #define LDAUX(k) ctx.ldaux(k)
 #define PREFETCH_ROW(gf, b, c) ctx.prefetch_row(gf, b, c)
+#define PREFETCH_ROW_L2(gf, b, c) ctx.prefetch_row_l2(gf, b, c)
 #define RFM(arr, d) __ldg(ctx.rfm.arr + ctx.i##d)
 #define rfm_f0 f0
 #define rfm_f0_D0 f0_D0
