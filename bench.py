@@ -291,6 +291,7 @@ def main():
     ap.add_argument("--no-diff", action="store_true", help="skip the adjoint-gradient section")
     ap.add_argument("--no-diag", action="store_true", help="skip the diagnostics-output section")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's own CUDA build")
+    ap.add_argument("--no-cyl", action="store_true", help="skip the SinhCylindrical (blackhole_spectroscopy grid) section")
     ap.add_argument("--diff-only", action="store_true",
                     help="run only the adjoint-gradient section (one GPU) and print it as JSON (profiling)")
     ap.add_argument("--batched-only", action="store_true",
@@ -412,6 +413,7 @@ def main():
     # measured at 4th order, its 8th-order test covering Nxx2 >= 4.
     batched = None if (args.no_batched or FD_ORDER != 4) else run_batched(args, world, rank, dist)
     differentiation = None if (args.no_diff or rank != 0 or FD_ORDER != 4) else run_differentiation()
+    cylindrical = None if (args.no_cyl or rank != 0) else run_cylindrical(args)
 
     if rank == 0:
         cpu = None
@@ -461,6 +463,7 @@ def main():
             "differentiation": differentiation,
             "diagnostics": diag,
             "checkpoint": ckpt,
+            "cylindrical": cylindrical,
         }
         print(json.dumps(line))
     if dist is not None:
@@ -658,6 +661,68 @@ def run_batched(args, world, rank, dist):
             "tile_fill": info["tile_fill"],
             "sequential_single_grid_value": seq_value,
             "speedup_vs_sequential": value / seq_value if seq_value else None}
+
+
+CYL_NXX = (400, 2, 1200)
+CYL_L = 300.0
+
+
+def run_cylindrical(args, steps: int = 20):
+    """SinhCylindrical, axisymmetric about z, on blackhole_spectroscopy.py's grid (400x2x1200,
+    AMPLRHO = AMPLZ = 300, SINHW 0.2) with this process's FD order and the bench's seeded
+    Brill-Lindquist data: `steps` fused FP64 RK4 steps replayed from one CUDA graph, timed with
+    CUDA events; beside it the reference's generated C of the same coordinates on the host
+    cores (2 warm-up steps, median of 3 runs of 2 steps)."""
+    import torch
+
+    from nrpy_b200.grid import BSSNGrid
+
+    m1, z1, m2, z2 = bl_params(args.seed)
+    g = BSSNGrid(coord="SinhCylindrical", Nxx=CYL_NXX, grid_physical_size=CYL_L, SINHW=SINHW, BH1_mass=m1,
+                 BH1_posn_z=z1, BH2_mass=m2, BH2_posn_z=z2, symmetry_axes="1")
+    st = g.make_stepper(mode=1, steps_per_graph=steps)
+    with torch.cuda.stream(st):
+        g.run_stepper(1)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    with torch.cuda.stream(st):
+        g.run_stepper(1)
+    b.record(st)
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    pts = CYL_NXX[0] * CYL_NXX[1] * CYL_NXX[2]
+    res = {"workload": f"SinhCylindrical {CYL_NXX[0]}x{CYL_NXX[1]}x{CYL_NXX[2]} (blackhole_spectroscopy's grid), "
+                       f"AMPLRHO = AMPLZ = {CYL_L:g}, SINHW {SINHW}, symmetry_axes '1', {FD_ORDER}th-order FD, "
+                       f"FP64 fused stages",
+           "value": pts * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps}
+    g.free_stepper()
+    g.close()
+    del g
+    torch.cuda.empty_cache()
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+
+            variant = "sinhcyl" if FD_ORDER == 4 else f"sinhcyl{FD_ORDER}"
+            if ref.available(variant):
+                rg = ref.RefGrid(variant, CYL_NXX, CYL_L, SINHW=SINHW, BH1_mass=m1, BH1_posn_z=z1, BH2_mass=m2,
+                                 BH2_posn_z=z2)
+                rg.step(2)
+                times = []
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    rg.step(2)
+                    times.append(time.perf_counter() - t0)
+                rg.close()
+                dt = float(np.median(times))
+                res["reference_value"] = pts * 2 / dt
+                res["reference_s_per_step"] = dt / 2
+                res["reference_cores"] = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+                res["speedup_vs_reference"] = res["value"] / res["reference_value"]
+        except Exception as e:  # noqa: BLE001
+            res["reference_unavailable"] = str(e)
+    return res
 
 
 def run_diagnostics(grid, args, reps: int = 3):

@@ -179,12 +179,22 @@ static dim3 interior_grid(const GridDims &g, int by = BY) {
 #endif
 constexpr int TX = BSSN_TILE_X, TZ = BSSN_TILE_Z;
 
-static dim3 group_block(int nt) { return dim3(TX, nt / (TX * TZ), TZ); }
+// A grid with fewer than NT / TX interior points along i1 (the axisymmetric SinhCylindrical
+// grid has 2 phi points) would leave block rows idle; there the block takes the remaining
+// threads along i2 instead (32 x 2 x 2 for 128 threads and 2 phi points).
+static dim3 group_block(const GridDims &g, int nt) {
+  const int n1 = g.N1 - 2 * NGHOSTS;
+  int ty = nt / (TX * TZ), tz = TZ;
+  while (ty > 1 && ty / 2 >= n1) {
+    ty /= 2;
+    tz *= 2;
+  }
+  return dim3(TX, ty, tz);
+}
 
-static dim3 group_grid(const GridDims &g, int nt) {
+static dim3 group_grid(const GridDims &g, const dim3 &blk) {
   const int n0 = g.N0 - 2 * NGHOSTS, n1 = g.N1 - 2 * NGHOSTS, n2 = g.N2 - 2 * NGHOSTS;
-  const int ty = nt / (TX * TZ);
-  return dim3((n0 + TX - 1) / TX, (n1 + ty - 1) / ty, (n2 + TZ - 1) / TZ);
+  return dim3((n0 + blk.x - 1) / blk.x, (n1 + blk.y - 1) / blk.y, (n2 + blk.z - 1) / blk.z);
 }
 
 #define GROUP_INDEX_OR_RETURN(g)                                        \
@@ -442,7 +452,8 @@ static int launch_ricci_group(const GridDims &g, const RfmArrays &rfm, const dou
   using Grp = RicciG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(ricci_kernel<V, G, T>, sb));
-  ricci_kernel<V, G, T><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, in, aux);
+  const dim3 blk = group_block(g, Grp::NT);
+  ricci_kernel<V, G, T><<<group_grid(g, blk), blk, sb, s>>>(g, rfm, in, aux);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -470,7 +481,8 @@ static int launch_rhs_group(const GridDims &g, const RfmArrays &rfm, const PhysP
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(rhs_kernel<V, T, G>, sb));
-  rhs_kernel<V, T, G><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, pp, aux, in, rhs);
+  const dim3 blk = group_block(g, Grp::NT);
+  rhs_kernel<V, T, G><<<group_grid(g, blk), blk, sb, s>>>(g, rfm, pp, aux, in, rhs);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
 }
@@ -523,7 +535,8 @@ static int launch_fused_group(const GridDims &g, const RfmArrays &rfm, const Phy
   using Grp = RhsG<V, G>;
   constexpr size_t sb = slot_bytes<Grp, T>();
   BSSN_TRY(set_smem(rhs_fused_kernel<V, T, STAGE, G>, sb));
-  rhs_fused_kernel<V, T, STAGE, G><<<group_grid(g, Grp::NT), group_block(Grp::NT), sb, s>>>(g, rfm, pp, aux, b,
+  const dim3 blk = group_block(g, Grp::NT);
+  rhs_fused_kernel<V, T, STAGE, G><<<group_grid(g, blk), blk, sb, s>>>(g, rfm, pp, aux, b,
                                                                                               krhs, dt);
   BSSN_LAUNCH_CHECK();
   return BSSN_B200_OK;
