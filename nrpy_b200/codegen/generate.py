@@ -400,6 +400,7 @@ def main() -> None:
     ap.add_argument("--prefetch-f64", default=None, help="tuning: the same for the FP64 groups")
     ap.add_argument("--prefetch-f64-l2", action="store_true", help="tuning: FP64 row prefetches into L2")
     ap.add_argument("--caps-f64", default=None, help="tuning: FP64 register budgets 'ricci0,ricci1,rhs0,rhs1'")
+    ap.add_argument("--caps-f32", default=None, help="tuning: the same for the FP32 groups")
     ap.add_argument("--one", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--one-adjoint", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -416,6 +417,10 @@ def main() -> None:
         d = [int(x) for x in args.caps_f64.split(",")]
         RICCI_CAPS[:] = d[:2]
         RHS_CAPS[:] = d[2:4]
+    if args.caps_f32:
+        d = [int(x) for x in args.caps_f32.split(",")]
+        RICCI_CAPS_F32[:] = d[:2]
+        RHS_CAPS_F32[:] = d[2:4]
     global PREFETCH_MACRO
     if args.prefetch_f64_l2:
         PREFETCH_MACRO = "PREFETCH_ROW_L2"
@@ -437,7 +442,8 @@ def main() -> None:
                           str(args.fd_order)] + (["--prefetch-f32", args.prefetch_f32] if args.prefetch_f32 else [])
                          + (["--prefetch-f64", args.prefetch_f64] if args.prefetch_f64 else [])
                          + (["--prefetch-f64-l2"] if args.prefetch_f64_l2 else [])
-                         + (["--caps-f64", args.caps_f64] if args.caps_f64 else []),
+                         + (["--caps-f64", args.caps_f64] if args.caps_f64 else [])
+                         + (["--caps-f32", args.caps_f32] if args.caps_f32 else []),
                          env=env, cwd=ROOT)
         for tag in args.variants.split(",") if tag
     ]
